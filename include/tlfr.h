@@ -1,0 +1,194 @@
+/*
+ * tlfr.h — C ABI of the B200 temporal light field reconstruction library
+ * (libtlfr.so).  Plain C types only: pointers, sizes, status codes.
+ *
+ * The entry points replace the reference reconstruction library's API
+ * (jiawen/temporal-lightfield-reconstruction, src/reconstruction_lib):
+ *
+ *   tlfr_buffer_load        UVTSampleBuffer::UVTSampleBuffer(const char*)      common/SampleBuffer.cpp:230-387
+ *   tlfr_buffer_from_host   UVTSampleBuffer filled in memory (App import path) reconstruction_app/App.cpp:334-433
+ *   tlfr_buffer_save        UVTSampleBuffer::serialize(...)                    common/SampleBuffer.cpp:404-564
+ *   tlfr_create             TreeGather::TreeGather(sbuf, params, aperture, focus)
+ *                                                                              reconstruction/Reconstruction.hpp:45,
+ *                                                                              reconstruction/Reconstruction.cpp:43-215
+ *   tlfr_reconstruct        TreeGather::reconstructDofMotion(Image&)           reconstruction/Reconstruction.cpp:221-295
+ *                           with CameraParams::enableCuda (the CPU/GPU toggle, Reconstruction.cpp:233) always "GPU"
+ *   tlfr_params             the CameraParams fields the path reads              common/CameraParams.hpp:74-107
+ *
+ * Error behaviour: the reference aborts through fail() (framework/base/Defs.hpp:142);
+ * every entry point here returns a tlfr_status instead and records a message
+ * retrievable with tlfr_last_error().  There is no CPU fallback: when the CUDA
+ * device or kernels are unavailable the calls fail with TLFR_CUDA / TLFR_NO_DEVICE.
+ *
+ * Threading: a context is externally synchronised (one host thread at a time).
+ * All device work of a context is issued on the stream given at creation; calls
+ * that return host data synchronise that stream.
+ */
+#ifndef TLFR_H
+#define TLFR_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tlfr_status
+{
+    TLFR_OK        = 0,
+    TLFR_BAD_ARG   = 1,   /* invalid argument (null pointer, bad size, unknown mode)     */
+    TLFR_IO        = 2,   /* file could not be opened / read / written                   */
+    TLFR_FORMAT    = 3,   /* unsupported header version or malformed records             */
+    TLFR_OOM       = 4,   /* device or host allocation failed                            */
+    TLFR_CUDA      = 5,   /* a CUDA call or kernel failed                                */
+    TLFR_OVERFLOW  = 6,   /* a query or build exceeded the largest supported capacity    */
+    TLFR_TIMEOUT   = 7,   /* a bounded device wait gave up                               */
+    TLFR_NO_DEVICE = 8,   /* no CUDA device                                              */
+    TLFR_EMPTY     = 9    /* every sample was discarded (Reconstruction.cpp:587-588)     */
+} tlfr_status;
+
+typedef struct tlfr_buffer tlfr_buffer;   /* host sample buffer (UVTSampleBuffer)      */
+typedef struct tlfr_ctx    tlfr_ctx;      /* device hierarchy + query state (TreeGather) */
+
+/* Lens/time output-sample weighting, CameraParams.hpp:48-58. */
+enum { TLFR_FILTER_BOX = 0, TLFR_FILTER_GAUSSIAN = 1 };
+
+/* Reconstruction parameters (the CameraParams fields the path reads). */
+typedef struct tlfr_params
+{
+    float aperture_adjust;   /* TreeGather ctor apertureAdjust, default 1 (Reconstruction.hpp:45) */
+    float focus_adjust;      /* TreeGather ctor focalDistanceAdjust, default 1                  */
+    int   lens_filter;       /* TLFR_FILTER_*, CameraParams::lensFilter                          */
+    int   time_filter;       /* TLFR_FILTER_*, CameraParams::timeFilter                          */
+    int   override_uvt;      /* nonzero: CameraParams::overrideUVT = uvt (one output sample per
+                                pixel at the pixel centre, Reconstruction.cpp:454-500);
+                                the t=1 pinhole image is uvt = {0,0,1} (App.cpp:450)           */
+    float uvt[3];
+    int   output_spp;        /* output samples per pixel; 0 = reference default (128, or 1 with
+                                override_uvt; Reconstruction.hpp:67-68).  Any value in [1,1024]. */
+    int   device;            /* CUDA device ordinal                                              */
+} tlfr_params;
+
+/* Fills p with the reference defaults (CameraParams ctor, CameraParams.hpp:77-90). */
+void tlfr_params_default(tlfr_params* p);
+
+/* Per-reconstruction counters.  The first eight follow TreeGather::Stats
+ * (Reconstruction.hpp:134-147), summed over all output samples; the rest are
+ * device-side query classes.                                                   */
+typedef struct tlfr_stats
+{
+    double num_output_samples;
+    double num_leaf_nodes;            /* leaves intersected, summed over fetch passes      */
+    double num_samples_in_leaf_nodes; /* samples tested, summed over fetch passes          */
+    double num_samples_within_1r;
+    double num_samples_fetched;       /* samples accepted, summed over fetch passes        */
+    double num_surfaces;
+    double num_2r;                    /* output samples that did a 2R fetch                */
+    double num_surfaces_merged;
+    double num_at_least_one;          /* output samples that widened beyond 2R             */
+    double num_overflow_queries;      /* queries re-run by the large-capacity pass          */
+    double num_empty;                 /* output samples that found no sample at all        */
+    double build_ms;                  /* device time of the last hierarchy build           */
+    double query_ms;                  /* device time of the last reconstruction            */
+} tlfr_stats;
+
+/* ---- sample buffers ------------------------------------------------------- */
+
+/* Load <path> (+ <path>.header when present), header version 1.3, text or binary
+ * 16-float records; alpha forced to 1 (SampleBuffer.cpp:343, 372).              */
+tlfr_status tlfr_buffer_load(const char* path, tlfr_buffer** out);
+
+/* Wrap host records (16 floats each, pixel-major, index (y*W+x)*spp+i, field order
+ * x,y,z/w,w,u,v,t,r,g,b,a,mv_x,mv_y,mv_w,dwdx,dwdy).  The records are copied;
+ * alpha is forced to 1 as the loader does.                                     */
+tlfr_status tlfr_buffer_from_host(const float* records16, int width, int height, int spp,
+                                  float coc0, float coc1, tlfr_buffer** out);
+
+/* Write a buffer in the reference format (SampleBuffer.cpp:404-564): header v1.3,
+ * separate "<path>.header" when separate_header, binary or text records.        */
+tlfr_status tlfr_buffer_save(const tlfr_buffer* buf, const char* path, int separate_header, int binary);
+
+tlfr_status  tlfr_buffer_info(const tlfr_buffer* buf, int* width, int* height, int* spp,
+                              float* coc0, float* coc1);
+const float* tlfr_buffer_records(const tlfr_buffer* buf);
+void         tlfr_buffer_free(tlfr_buffer* buf);
+
+/* ---- hierarchy build and reconstruction ------------------------------------ */
+
+/* TreeGather ctor: upload the buffer and build the 5D sample hierarchy on the GPU.
+ * stream: a cudaStream_t (NULL = the legacy default stream).                     */
+tlfr_status tlfr_create(const tlfr_buffer* buf, const tlfr_params* params, void* stream, tlfr_ctx** out);
+
+/* Same, from records already in device memory (16 floats each, layout as above). */
+tlfr_status tlfr_create_device(const float* d_records16, int width, int height, int spp,
+                               float coc0, float coc1, const tlfr_params* params, void* stream,
+                               tlfr_ctx** out);
+
+/* Rebuild the hierarchy of an existing context from new device records of the same
+ * size, reusing its device memory (no allocation when the sizes still fit).       */
+tlfr_status tlfr_rebuild_device(tlfr_ctx* ctx, const float* d_records16);
+
+/* reconstructDofMotion: one RGBA float pixel per buffer pixel, row-major, alpha 1,
+ * (1,0,0,1) where no sample was found (Reconstruction.cpp:716-719).
+ * rgba_on_device: 0 = rgba is host memory (the call synchronises), 1 = device memory
+ * (the call returns once the work is queued on the context's stream).
+ * stats may be NULL.                                                              */
+tlfr_status tlfr_reconstruct(tlfr_ctx* ctx, float* rgba, int rgba_on_device, tlfr_stats* stats);
+
+/* Change the output-sample parameters (override_uvt/uvt, output_spp, filters) of an
+ * existing context; the hierarchy is kept (App.cpp:616-694 refocus/animation loop). */
+tlfr_status tlfr_set_output(tlfr_ctx* ctx, const tlfr_params* params);
+
+tlfr_status tlfr_sync(tlfr_ctx* ctx);
+tlfr_status tlfr_get_stats(tlfr_ctx* ctx, tlfr_stats* stats);
+void        tlfr_destroy(tlfr_ctx* ctx);
+
+/* Message of the last failed call on ctx (ctx may be NULL for creation errors). */
+const char* tlfr_last_error(const tlfr_ctx* ctx);
+
+/* ---- introspection (parity tests, profiling) -------------------------------- */
+
+/* Sizes of the built hierarchy.  nodes: hierarchy nodes; samples: samples stored in
+ * leaves (TreeGather::m_samples); height: longest root-to-leaf path.              */
+tlfr_status tlfr_tree_info(tlfr_ctx* ctx, int* num_nodes, int* num_samples, int* root, int* height);
+
+/* Copy the hierarchy to host memory.  Node i: nodef[i*14 .. +14) = 4 planes
+ * (xmin,xmax,ymin,ymax) as (t, uv, const) then tspan (2); nodei[i*5 .. +5) =
+ * child0, child1, s0, s1, ns (child0 == -1 for leaves; s0/s1 == -1 for internal
+ * nodes).  Sample j: samplef[j*12 .. +12) = x, y, w, t, mv(3), rgba(4), key;
+ * sample_ids[j] = index of the input record it came from.  Any pointer may be NULL. */
+tlfr_status tlfr_tree_export(tlfr_ctx* ctx, float* nodef, int* nodei, float* samplef, int* sample_ids);
+
+/* Output sampling pattern: 64 patterns x output_spp entries of (x, y, u, v, t)
+ * (generateOutputSamples, Reconstruction.cpp:452-512).  Returns the entry count.  */
+int tlfr_output_samples(tlfr_ctx* ctx, float* out5);
+
+/* Run the output samples (x, y, i) listed in xyi[3*k ..] through the device query
+ * path with tracing on.  rgba[4*k ..] = the query colour.  trace[k*trace_stride ..]:
+ *   [0] flags: bit0 = 2R fetch, bit1 = widened beyond 2R, bit2 = surfaces merged,
+ *       bit3 = ran in the large-capacity pass
+ *   [1] S = number of surfaces after the final fetch and tiny-surface merging,
+ *   then per surface: n, minIndex, n sample indices (into the hierarchy's samples).
+ * A trace that does not fit its stride is cut and its [1] set to -1.             */
+tlfr_status tlfr_trace_queries(tlfr_ctx* ctx, const int* xyi, int num_queries,
+                               float* rgba, int* trace, int trace_stride);
+
+/* ---- synthetic scenes (tests, benchmarks) ---------------------------------- */
+
+enum
+{
+    TLFR_SCENE_PLANES      = 0,   /* three fronto-parallel planes at w=2,5,12; defocus only       */
+    TLFR_SCENE_CARDS       = 1,   /* 64 moving textured rectangles, w in [1,50]; defocus + motion */
+    TLFR_SCENE_CARDS_LARGE = 2    /* 256 rectangles + 64 disks, w in [0.5,100]; strong blur       */
+};
+
+/* Fill records (width*height*spp*16 floats) with a seeded analytic scene; coc_out
+ * receives (C0, C1).  Host-side, multithreaded, deterministic for a given seed.   */
+tlfr_status tlfr_synth_scene(int preset, int width, int height, int spp, unsigned long long seed,
+                             float* records, float* coc_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TLFR_H */
