@@ -1,0 +1,864 @@
+// tlfr_api.cpp — the C ABI (include/tlfr.h): sample-buffer IO, the output
+// sampling pattern, context lifetime, and the calls into the CUDA build and
+// query code.  Host code; compiled with -ffp-contract=off so that the pattern
+// arithmetic matches the reference's IEEE single-precision host code.
+#include "tlfr.h"
+#include "tlfr_common.cuh"
+#include "tlfr_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+struct tlfr_buffer
+{
+    int W = 0, H = 0, spp = 0;
+    float coc[2] = { 0, 0 };
+    std::vector<float> rec;     // W*H*spp*16
+};
+
+struct tlfr_ctx
+{
+    tlfr::Ctx c;
+    bool own_stream = false;
+};
+
+namespace
+{
+
+thread_local std::string g_create_error;
+
+tlfr_status fail(tlfr_ctx* ctx, tlfr_status s, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->c.error = buf;
+    else     g_create_error = buf;
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Text record parsing: the framework's float parser (framework/base/String.cpp:
+// 428-480) accumulates digits in single precision and scales the exponent with
+// powf; text buffers load bit-identically only through the same steps.
+// ---------------------------------------------------------------------------
+bool parse_float(const char*& ptr, float& value)
+{
+    const char* tmp = ptr;
+    bool neg = false;
+    if (*tmp == '+') tmp++;
+    else if (*tmp == '-') { neg = true; tmp++; }
+    float v = 0.0f;
+    int digits = 0;
+    while (*tmp >= '0' && *tmp <= '9')
+    {
+        v = v * 10.0f + (float)(*tmp++ - '0');
+        digits++;
+    }
+    if (*tmp == '.')
+    {
+        tmp++;
+        float scale = 1.0f;
+        while (*tmp >= '0' && *tmp <= '9')
+        {
+            scale *= 0.1f;
+            v += scale * (float)(*tmp++ - '0');
+            digits++;
+        }
+    }
+    if (!digits)
+        return false;
+    ptr = tmp;
+    if (*ptr == '#')
+    {
+        struct { const char* lit; uint32_t pos, neg; } specials[] = {
+            { "#INF", 0x7F800000u, 0xFF800000u }, { "#SNAN", 0x7F800001u, 0xFF800001u },
+            { "#QNAN", 0x7FC00001u, 0xFFC00001u }, { "#IND", 0x7FC00000u, 0xFFC00000u } };
+        for (auto& sp : specials)
+        {
+            size_t L = strlen(sp.lit);
+            if (strncmp(ptr, sp.lit, L) == 0)
+            {
+                ptr += L;
+                uint32_t bits = neg ? sp.neg : sp.pos;
+                memcpy(&value, &bits, 4);
+                return true;
+            }
+        }
+    }
+    if (*tmp == 'e' || *tmp == 'E')
+    {
+        const char* t2 = tmp + 1;
+        bool eneg = false;
+        if (*t2 == '+') t2++;
+        else if (*t2 == '-') { eneg = true; t2++; }
+        if (*t2 >= '0' && *t2 <= '9')
+        {
+            int e = 0;
+            while (*t2 >= '0' && *t2 <= '9')
+                e = e * 10 + (*t2++ - '0');
+            if (eneg) e = -e;
+            ptr = t2;
+            if (e)
+                v *= powf(10.0f, (float)e);
+        }
+    }
+    value = neg ? -v : v;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Output sampling pattern (Reconstruction.cpp:452-512) and the sequences it
+// uses (reconstruction_lib/common/Util.cpp:37-74, 229-300;
+// framework/base/Random.cpp:52-92).
+// ---------------------------------------------------------------------------
+struct Ranrot
+{
+    int32_t p1, p2;
+    uint32_t buf[11];
+    explicit Ranrot(uint32_t seed)
+    {
+        if (seed == 0) seed--;
+        for (int i = 0; i < 11; i++)
+        {
+            seed ^= seed << 13;
+            seed ^= seed >> 17;
+            seed ^= seed << 5;
+            buf[i] = seed;
+        }
+        p1 = 0; p2 = 7;
+        for (int i = 0; i < 11; i++) next();
+    }
+    uint32_t next()
+    {
+        uint32_t x = buf[p1] + buf[p2];
+        x = (x << 13) | (x >> 19);
+        buf[p1] = x;
+        p1--; p1 += (p1 >> 31) & 11;
+        p2--; p2 += (p2 >> 31) & 11;
+        return x;
+    }
+    float f32() { return (float)next() * (1.0f / 4294967296.0f); }
+};
+
+float hammersley(int i, int num) { return ((float)i + 0.5f) / (float)num; }
+
+float halton(int base, int i)
+{
+    float h = 0.0f;
+    float half = tlfr::rcp((float)base);
+    while (i)
+    {
+        int digit = i % base;
+        h = h + (float)digit * half;
+        i = (i - digit) / base;
+        half = half / (float)base;
+    }
+    return h;
+}
+
+// Sobol dimension 3: primitive polynomial x^3 + x + 1, initial direction
+// numbers m = (1, 3, 1).
+float sobol_dim3(int i)
+{
+    static uint32_t v[32];
+    static bool init = false;
+    if (!init)
+    {
+        v[0] = 1u << 31; v[1] = 3u << 30; v[2] = 1u << 29;
+        for (int k = 3; k < 32; k++)
+            v[k] = v[k - 2] ^ v[k - 3] ^ (v[k - 3] >> 3);
+        init = true;
+    }
+    uint32_t r = 0;
+    for (unsigned c = 0; i; i >>= 1, ++c)
+        if (i & 1) r ^= v[c];
+    return (float)r * (1.0f / 4294967296.0f);
+}
+
+void sobol_2d(int i, float* out)
+{
+    uint32_t r1 = 0, r2 = 0;
+    for (uint32_t v1 = 1u << 31, v2 = 3u << 30; i; i >>= 1)
+    {
+        if (i & 1) { r1 ^= v1; r2 ^= v2 << 1; }
+        v1 |= v1 >> 1;
+        v2 ^= v2 >> 1;
+    }
+    out[0] = (float)r1 * (1.0f / 4294967296.0f);
+    out[1] = (float)r2 * (1.0f / 4294967296.0f);
+}
+
+float larcher_pillichshammer(int i)
+{
+    uint32_t r = 0;
+    for (uint32_t v = 1u << 31; i; i >>= 1, v |= v >> 1)
+        if (i & 1) r ^= v;
+    return (float)((double)r / (double)0x100000000LL);
+}
+
+// Shirley-Chiu concentric square-to-disk map
+void to_unit_disk(float sx, float sy, float& ou, float& ov)
+{
+    const float PI = 3.1415926535897932384626433832795f;
+    float phi, r;
+    float a = 2.0f * sx - 1.0f;
+    float b = 2.0f * sy - 1.0f;
+    if (a > -b)
+    {
+        if (a > b) { r = a; phi = (PI / 4) * (b / a); }
+        else       { r = b; phi = (PI / 4) * (2.0f - (a / b)); }
+    }
+    else
+    {
+        if (a < b) { r = -a; phi = (PI / 4) * (4.0f + (b / a)); }
+        else
+        {
+            r = -b;
+            phi = (b != 0) ? (PI / 4) * (6.0f - (a / b)) : 0.0f;
+        }
+    }
+    ou = r * cosf(phi);
+    ov = r * sinf(phi);
+}
+
+struct PatSample { float x, y, u, v, t, key; };
+
+struct KeySort
+{
+    PatSample* e;
+    int cmp(int a, int b) const { return (e[a].key < e[b].key) ? -1 : (e[a].key > e[b].key) ? 1 : 0; }
+    void swap(int a, int b) { PatSample t = e[a]; e[a] = e[b]; e[b] = t; }
+};
+
+} // namespace
+
+namespace tlfr
+{
+
+void generate_output_pattern(int M, bool override_uvt, const float* uvt, std::vector<float>& out5)
+{
+    Ranrot rnd(242);
+    std::vector<PatSample> all((size_t)64 * M);
+    for (int j = 0; j < 64; j++)
+    {
+        const float xo[2] = { hammersley(j, 64), larcher_pillichshammer(j) };
+        const float uo[2] = { halton(2, j), halton(3, j) };
+        const float tj = rnd.f32();
+        PatSample* p = &all[(size_t)j * M];
+        for (int i = 0; i < M; i++)
+        {
+            float s2[2];
+            sobol_2d(i + 1, s2);
+            float x = sobol_dim3(i + 1);
+            float y = larcher_pillichshammer(i + 1);
+            float t = ((float)i + tj) / (float)M;
+            float xy[2] = { x + xo[0], y + xo[1] };
+            float uv[2] = { s2[0] + uo[0], s2[1] + uo[1] };
+            if (xy[0] >= 1.f) xy[0] -= 1.f;
+            if (xy[1] >= 1.f) xy[1] -= 1.f;
+            if (uv[0] >= 1.f) uv[0] -= 1.f;
+            if (uv[1] >= 1.f) uv[1] -= 1.f;
+            // (u,v,t) Morton key for coherence (Reconstruction.cpp:482-489)
+            int ub = (int)floorf(256.0f * uv[0]);
+            int vb = (int)floorf(256.0f * uv[1]);
+            int tb = (int)floorf(256.0f * t);
+            int key = 0;
+            for (int k = 0; k < 8; k++)
+                key |= ((ub >> k) & 1) << (3 * k + 2) | ((vb >> k) & 1) << (3 * k + 1) | ((tb >> k) & 1) << (3 * k + 0);
+            to_unit_disk(uv[0], uv[1], uv[0], uv[1]);
+            if (override_uvt)
+            {
+                uv[0] = uvt[0]; uv[1] = uvt[1];
+                t = uvt[2];
+            }
+            if (M == 1)
+                xy[0] = xy[1] = 0.5f;
+            p[i] = PatSample{ xy[0], xy[1], uv[0], uv[1], t, (float)key };
+        }
+        KeySort ks{ p };
+        fw_sort(ks, 0, M);
+    }
+    out5.resize((size_t)64 * M * 5);
+    for (size_t k = 0; k < all.size(); k++)
+    {
+        out5[k * 5 + 0] = all[k].x; out5[k * 5 + 1] = all[k].y;
+        out5[k * 5 + 2] = all[k].u; out5[k * 5 + 3] = all[k].v;
+        out5[k * 5 + 4] = all[k].t;
+    }
+}
+
+} // namespace tlfr
+
+namespace
+{
+
+tlfr_status upload_pattern(tlfr_ctx* ctx)
+{
+    tlfr::Ctx& c = ctx->c;
+    const bool ov = c.params.override_uvt != 0;
+    c.out_spp = c.params.output_spp > 0 ? c.params.output_spp : (ov ? 1 : 128);
+    if (c.out_spp > 1024)
+        return fail(ctx, TLFR_BAD_ARG, "output_spp %d out of range [1,1024]", c.out_spp);
+    tlfr::generate_output_pattern(c.out_spp, ov, c.params.uvt, c.h_pattern);
+    if (c.d_pattern) cudaFree(c.d_pattern);
+    c.d_pattern = nullptr;
+    cudaError_t e = cudaMalloc(&c.d_pattern, sizeof(float) * c.h_pattern.size());
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_OOM, "pattern allocation: %s", cudaGetErrorString(e));
+    e = cudaMemcpyAsync(c.d_pattern, c.h_pattern.data(), sizeof(float) * c.h_pattern.size(), cudaMemcpyHostToDevice,
+                        c.stream);
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "pattern upload: %s", cudaGetErrorString(e));
+    return TLFR_OK;
+}
+
+void free_ctx_buffers(tlfr::Ctx& c)
+{
+    void* ptrs[] = { c.own_records ? c.d_records : nullptr, c.rp_pos, c.rp_mot, c.rp_cell, c.hits, c.d_grid,
+                     c.cell_count, c.cell_start, c.cell_items, c.kd, c.kd_level, c.kd_leaves_ordered, c.perm, c.box,
+                     c.sbounds, c.surface, c.pending, c.leaf_task_rank, c.ordered_n, c.ordered_prefmax, c.top,
+                     c.nodes, c.node_tspan, c.s_pos, c.s_mot, c.s_col, c.s_id, c.d_pattern, c.accum, c.ovf_queue,
+                     c.ovf_scratch, c.d_stats, c.d_out };
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c.ev0) cudaEventDestroy(c.ev0);
+    if (c.ev1) cudaEventDestroy(c.ev1);
+    if (c.ev2) cudaEventDestroy(c.ev2);
+}
+
+tlfr_status begin_ctx(const tlfr_params* params, void* stream, int W, int H, int spp, float c0, float c1,
+                      tlfr_ctx** out, tlfr_ctx*& ctx)
+{
+    if (!out || W <= 0 || H <= 0 || spp <= 0)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_create: bad argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    {
+        cudaGetLastError();
+        return fail(nullptr, TLFR_NO_DEVICE, "no CUDA device");
+    }
+    ctx = new (std::nothrow) tlfr_ctx();
+    if (!ctx)
+        return fail(nullptr, TLFR_OOM, "host allocation failed");
+    tlfr::Ctx& c = ctx->c;
+    if (params) c.params = *params;
+    else        tlfr_params_default(&c.params);
+    if (c.params.device < 0 || c.params.device >= ndev)
+        return fail(ctx, TLFR_BAD_ARG, "device %d out of range", c.params.device);
+    c.device = c.params.device;
+    cudaError_t e = cudaSetDevice(c.device);
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    c.stream = (cudaStream_t)stream;
+    c.W = W; c.H = H; c.spp_in = spp;
+    c.n_in = (size_t)W * H * spp;
+    c.coc0_raw[0] = c0; c.coc0_raw[1] = c1;
+    // refocus round trip (Reconstruction.cpp:77-87)
+    {
+        float a = -c0;
+        float f = (-c0) * tlfr::rcp(c1);
+        a *= c.params.aperture_adjust;
+        f *= c.params.focus_adjust;
+        c.coc[0] = -a;
+        c.coc[1] = a * tlfr::rcp(f);
+    }
+    // m_spp: next power of two (Reconstruction.cpp:63-73, Util.hpp:64-73)
+    uint32_t v = (uint32_t)spp;
+    v--; v |= v >> 1; v |= v >> 2; v |= v >> 4; v |= v >> 8; v |= v >> 16;
+    c.spp = tlfr::maxi(1, (int)(v + 1));
+    if (c.spp > 256)
+        return fail(ctx, TLFR_BAD_ARG, "TreeGather::Filterer::reconstruct -- unknown SPP (%d)", spp);
+    if (cudaEventCreate(&c.ev0) != cudaSuccess || cudaEventCreate(&c.ev1) != cudaSuccess ||
+        cudaEventCreate(&c.ev2) != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "cudaEventCreate failed");
+    tlfr_status st = upload_pattern(ctx);
+    if (st != TLFR_OK)
+        return st;
+    *out = nullptr;
+    return TLFR_OK;
+}
+
+tlfr_status run_build(tlfr_ctx* ctx, const float* d_rec)
+{
+    tlfr::Ctx& c = ctx->c;
+    cudaEventRecord(c.ev0, c.stream);
+    tlfr_status st = tlfr::build_hierarchy(c, d_rec);
+    if (st != TLFR_OK)
+        return st;
+    cudaEventRecord(c.ev1, c.stream);
+    cudaError_t e = cudaEventSynchronize(c.ev1);
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "build: %s", cudaGetErrorString(e));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c.ev0, c.ev1);
+    c.last.build_ms = ms;
+    return TLFR_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+void tlfr_params_default(tlfr_params* p)
+{
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->aperture_adjust = 1.0f;
+    p->focus_adjust = 1.0f;
+    p->lens_filter = TLFR_FILTER_BOX;
+    p->time_filter = TLFR_FILTER_BOX;
+    p->override_uvt = 0;
+    p->output_spp = 0;
+    p->device = 0;
+}
+
+tlfr_status tlfr_buffer_from_host(const float* rec, int W, int H, int spp, float c0, float c1, tlfr_buffer** out)
+{
+    if (!rec || !out || W <= 0 || H <= 0 || spp <= 0)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_buffer_from_host: bad argument");
+    tlfr_buffer* b = new (std::nothrow) tlfr_buffer();
+    if (!b)
+        return fail(nullptr, TLFR_OOM, "host allocation failed");
+    b->W = W; b->H = H; b->spp = spp;
+    b->coc[0] = c0; b->coc[1] = c1;
+    const size_t n = (size_t)W * H * spp;
+    try { b->rec.assign(rec, rec + n * 16); }
+    catch (...) { delete b; return fail(nullptr, TLFR_OOM, "host allocation failed"); }
+    for (size_t k = 0; k < n; k++)
+        b->rec[k * 16 + 10] = 1.0f;     // alpha forced to 1 (SampleBuffer.cpp:343, 372)
+    *out = b;
+    return TLFR_OK;
+}
+
+// UVTSampleBuffer(const char*) (SampleBuffer.cpp:230-387)
+tlfr_status tlfr_buffer_load(const char* path, tlfr_buffer** out)
+{
+    if (!path || !out)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_buffer_load: bad argument");
+    FILE* fp = fopen(path, "rb");
+    if (!fp)
+        return fail(nullptr, TLFR_IO, "File not found: %s", path);
+    std::string hp = std::string(path) + ".header";
+    FILE* fph = fopen(hp.c_str(), "rt");
+    const bool separate = fph != nullptr;
+    if (!separate)
+        fph = fp;
+    tlfr_buffer* b = new (std::nothrow) tlfr_buffer();
+    auto cleanup = [&]() { fclose(fp); if (separate) fclose(fph); };
+    float version = 0;
+    int W = 0, H = 0, spp = 0;
+    if (fscanf(fph, "Version %f\n", &version) != 1 || fscanf(fph, "Width %d\n", &W) != 1 ||
+        fscanf(fph, "Height %d\n", &H) != 1 || fscanf(fph, "Samples per pixel %d\n", &spp) != 1)
+    {
+        cleanup(); delete b;
+        return fail(nullptr, TLFR_FORMAT, "malformed sample buffer header: %s", path);
+    }
+    if (version != 1.3f)
+    {
+        cleanup(); delete b;
+        return fail(nullptr, TLFR_FORMAT, "Unsupported sample stream version (%.1f)", version);
+    }
+    if (W <= 0 || H <= 0 || spp <= 0 || (double)W * H * spp > 2.0e9)
+    {
+        cleanup(); delete b;
+        return fail(nullptr, TLFR_FORMAT, "bad buffer size %dx%dx%d", W, H, spp);
+    }
+    char motion[1024], enc[1024], desc[1024];
+    if (fscanf(fph, "Motion model: %1023s\n", motion) != 1) { /* optional line, as in the reference */ }
+    float c0 = 0, c1 = 0;
+    if (fscanf(fph, "CoC coefficients (coc radius = C0/w+C1): %f,%f\n", &c0, &c1) != 2)
+    {
+        cleanup(); delete b;
+        return fail(nullptr, TLFR_FORMAT, "missing CoC coefficients in header");
+    }
+    bool binary = false;
+    if (fscanf(fph, "Encoding = %1023s\n", enc) == 1)
+        binary = strcmp(enc, "binary") == 0;
+    if (fscanf(fph, "\n") < 0) {}
+    if (fscanf(fph, "%1023s\n", desc) != 1) {}
+    b->W = W; b->H = H; b->spp = spp; b->coc[0] = c0; b->coc[1] = c1;
+    const size_t n = (size_t)W * H * spp;
+    try { b->rec.assign(n * 16, 0.0f); }
+    catch (...) { cleanup(); delete b; return fail(nullptr, TLFR_OOM, "host allocation failed"); }
+    if (binary)
+    {
+        size_t got = fread(b->rec.data(), 64, n, fp);
+        if (got != n)
+        {
+            cleanup(); delete b;
+            return fail(nullptr, TLFR_FORMAT, "truncated binary records (%zu of %zu)", got, n);
+        }
+    }
+    else
+    {
+        std::vector<char> line(4096);
+        for (size_t k = 0; k < n; k++)
+        {
+            if (!fgets(line.data(), 4096, fp))
+            {
+                cleanup(); delete b;
+                return fail(nullptr, TLFR_FORMAT, "truncated text records (%zu of %zu)", k, n);
+            }
+            const char* p = line.data();
+            float* e = &b->rec[k * 16];
+            for (int v = 0; v < 16; v++)
+            {
+                if (v > 0)
+                {
+                    while (*p != ',' && *p != '\n' && *p != '\0') p++;
+                    if (*p) p++;
+                }
+                float val = 0.0f;
+                if (!parse_float(p, val))
+                    val = 0.0f;     // the reference leaves the value unset here
+                e[v] = val;
+            }
+        }
+    }
+    for (size_t k = 0; k < n; k++)
+        b->rec[k * 16 + 10] = 1.0f;
+    cleanup();
+    *out = b;
+    return TLFR_OK;
+}
+
+// UVTSampleBuffer::serialize (SampleBuffer.cpp:404-564), version 1.3.  As in the
+// reference the alpha field is written with the blue channel, and binary
+// output needs a separate header.
+tlfr_status tlfr_buffer_save(const tlfr_buffer* b, const char* path, int separate_header, int binary)
+{
+    if (!b || !path)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_buffer_save: bad argument");
+    if (binary && !separate_header)
+        return fail(nullptr, TLFR_BAD_ARG, "binary serialization supported only with a separate header");
+    FILE* fp = fopen(path, binary ? "wb" : "wt");
+    if (!fp)
+        return fail(nullptr, TLFR_IO, "cannot open %s", path);
+    FILE* fph = fp;
+    if (separate_header)
+    {
+        fph = fopen((std::string(path) + ".header").c_str(), "wt");
+        if (!fph) { fclose(fp); return fail(nullptr, TLFR_IO, "cannot open %s.header", path); }
+    }
+    fprintf(fph, "Version 1.3\n");
+    fprintf(fph, "Width %d\n", b->W);
+    fprintf(fph, "Height %d\n", b->H);
+    fprintf(fph, "Samples per pixel %d\n", b->spp);
+    fprintf(fph, "CoC coefficients (coc radius = C0/w+C1): %f,%f\n", b->coc[0], b->coc[1]);
+    fprintf(fph, "Encoding = %s\n", binary ? "binary" : "text");
+    fprintf(fph, "x,y,z/w,w,u,v,t,r,g,b,a,mv_x,mv_y,mv_w,dwdx,dwdy\n");
+    const size_t n = (size_t)b->W * b->H * b->spp;
+    bool ok = true;
+    if (binary)
+    {
+        std::vector<float> tmp(b->rec);
+        for (size_t k = 0; k < n; k++)
+            tmp[k * 16 + 10] = tmp[k * 16 + 9];
+        ok = fwrite(tmp.data(), 64, n, fp) == n;
+    }
+    else
+    {
+        for (size_t k = 0; k < n && ok; k++)
+        {
+            const float* e = &b->rec[k * 16];
+            for (int v = 0; v < 16; v++)
+                fprintf(fp, "%f,", (v == 10) ? e[9] : e[v]);
+            fprintf(fp, "\n");
+        }
+        ok = !ferror(fp);
+    }
+    fflush(fp);
+    fclose(fp);
+    if (separate_header) { fflush(fph); fclose(fph); }
+    return ok ? TLFR_OK : fail(nullptr, TLFR_IO, "write failed: %s", path);
+}
+
+tlfr_status tlfr_buffer_info(const tlfr_buffer* b, int* W, int* H, int* spp, float* c0, float* c1)
+{
+    if (!b)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_buffer_info: null buffer");
+    if (W) *W = b->W;
+    if (H) *H = b->H;
+    if (spp) *spp = b->spp;
+    if (c0) *c0 = b->coc[0];
+    if (c1) *c1 = b->coc[1];
+    return TLFR_OK;
+}
+
+const float* tlfr_buffer_records(const tlfr_buffer* b) { return b ? b->rec.data() : nullptr; }
+void tlfr_buffer_free(tlfr_buffer* b) { delete b; }
+
+tlfr_status tlfr_create(const tlfr_buffer* buf, const tlfr_params* params, void* stream, tlfr_ctx** out)
+{
+    if (!buf || !out)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_create: bad argument");
+    tlfr_ctx* ctx = nullptr;
+    tlfr_status st = begin_ctx(params, stream, buf->W, buf->H, buf->spp, buf->coc[0], buf->coc[1], out, ctx);
+    if (st != TLFR_OK)
+    {
+        if (ctx) { g_create_error = ctx->c.error; free_ctx_buffers(ctx->c); delete ctx; }
+        return st;
+    }
+    tlfr::Ctx& c = ctx->c;
+    cudaError_t e = cudaMalloc(&c.d_records, sizeof(float) * 16 * c.n_in);
+    if (e == cudaSuccess)
+    {
+        c.own_records = true;
+        e = cudaMemcpyAsync(c.d_records, buf->rec.data(), sizeof(float) * 16 * c.n_in, cudaMemcpyHostToDevice, c.stream);
+    }
+    if (e != cudaSuccess)
+    {
+        g_create_error = std::string("record upload: ") + cudaGetErrorString(e);
+        free_ctx_buffers(c); delete ctx;
+        return e == cudaErrorMemoryAllocation ? TLFR_OOM : TLFR_CUDA;
+    }
+    st = run_build(ctx, c.d_records);
+    if (st != TLFR_OK)
+    {
+        g_create_error = c.error;
+        free_ctx_buffers(c); delete ctx;
+        return st;
+    }
+    *out = ctx;
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_create_device(const float* d_rec, int W, int H, int spp, float c0, float c1,
+                               const tlfr_params* params, void* stream, tlfr_ctx** out)
+{
+    if (!d_rec || !out)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_create_device: bad argument");
+    tlfr_ctx* ctx = nullptr;
+    tlfr_status st = begin_ctx(params, stream, W, H, spp, c0, c1, out, ctx);
+    if (st != TLFR_OK)
+    {
+        if (ctx) { g_create_error = ctx->c.error; free_ctx_buffers(ctx->c); delete ctx; }
+        return st;
+    }
+    st = run_build(ctx, d_rec);
+    if (st != TLFR_OK)
+    {
+        g_create_error = ctx->c.error;
+        free_ctx_buffers(ctx->c); delete ctx;
+        return st;
+    }
+    *out = ctx;
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_rebuild_device(tlfr_ctx* ctx, const float* d_rec)
+{
+    if (!ctx || !d_rec)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_rebuild_device: bad argument");
+    cudaSetDevice(ctx->c.device);
+    return run_build(ctx, d_rec);
+}
+
+tlfr_status tlfr_reconstruct(tlfr_ctx* ctx, float* rgba, int rgba_on_device, tlfr_stats* stats)
+{
+    if (!ctx || !rgba)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_reconstruct: bad argument");
+    tlfr::Ctx& c = ctx->c;
+    cudaSetDevice(c.device);
+    const size_t npix = (size_t)c.W * c.H;
+    float4* dst = reinterpret_cast<float4*>(rgba);
+    if (!rgba_on_device)
+    {
+        if (!c.d_out)
+        {
+            cudaError_t e = cudaMalloc(&c.d_out, sizeof(float4) * npix);
+            if (e != cudaSuccess)
+                return fail(ctx, TLFR_OOM, "output allocation: %s", cudaGetErrorString(e));
+        }
+        dst = c.d_out;
+    }
+    cudaEventRecord(c.ev1, c.stream);
+    tlfr_status st = tlfr::reconstruct_frame(c, dst, stats != nullptr);
+    cudaEventRecord(c.ev2, c.stream);
+    if (st != TLFR_OK)
+        return st;
+    if (!rgba_on_device)
+    {
+        cudaError_t e = cudaMemcpyAsync(rgba, dst, sizeof(float4) * npix, cudaMemcpyDeviceToHost, c.stream);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(c.stream);
+        if (e != cudaSuccess)
+            return fail(ctx, TLFR_CUDA, "reconstruct: %s", cudaGetErrorString(e));
+    }
+    if (stats)
+    {
+        cudaError_t e = cudaEventSynchronize(c.ev2);
+        if (e != cudaSuccess)
+            return fail(ctx, TLFR_CUDA, "reconstruct: %s", cudaGetErrorString(e));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c.ev1, c.ev2);
+        c.last.query_ms = ms;
+        *stats = c.last;
+    }
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_set_output(tlfr_ctx* ctx, const tlfr_params* params)
+{
+    if (!ctx || !params)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_set_output: bad argument");
+    cudaSetDevice(ctx->c.device);
+    ctx->c.params.override_uvt = params->override_uvt;
+    memcpy(ctx->c.params.uvt, params->uvt, sizeof(params->uvt));
+    ctx->c.params.output_spp = params->output_spp;
+    ctx->c.params.lens_filter = params->lens_filter;
+    ctx->c.params.time_filter = params->time_filter;
+    return upload_pattern(ctx);
+}
+
+tlfr_status tlfr_sync(tlfr_ctx* ctx)
+{
+    if (!ctx)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_sync: null context");
+    cudaError_t e = cudaStreamSynchronize(ctx->c.stream);
+    return e == cudaSuccess ? TLFR_OK : fail(ctx, TLFR_CUDA, "%s", cudaGetErrorString(e));
+}
+
+tlfr_status tlfr_get_stats(tlfr_ctx* ctx, tlfr_stats* stats)
+{
+    if (!ctx || !stats)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_get_stats: bad argument");
+    *stats = ctx->c.last;
+    return TLFR_OK;
+}
+
+void tlfr_destroy(tlfr_ctx* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    free_ctx_buffers(ctx->c);
+    delete ctx;
+}
+
+const char* tlfr_last_error(const tlfr_ctx* ctx)
+{
+    return ctx ? ctx->c.error.c_str() : g_create_error.c_str();
+}
+
+tlfr_status tlfr_tree_info(tlfr_ctx* ctx, int* num_nodes, int* num_samples, int* root, int* height)
+{
+    if (!ctx)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_tree_info: null context");
+    if (num_nodes) *num_nodes = ctx->c.num_nodes;
+    if (num_samples) *num_samples = ctx->c.num_samples;
+    if (root) *root = ctx->c.root;
+    if (height) *height = ctx->c.height;
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_tree_export(tlfr_ctx* ctx, float* nodef, int* nodei, float* samplef, int* sample_ids)
+{
+    if (!ctx)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_tree_export: null context");
+    tlfr::Ctx& c = ctx->c;
+    cudaSetDevice(c.device);
+    const int nn = c.num_nodes, ns = c.num_samples;
+    std::vector<tlfr::QNode> q(nn);
+    std::vector<float2> ts(nn);
+    std::vector<float4> p(ns), m(ns), col(ns);
+    std::vector<int> id(ns);
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMemcpy(q.data(), c.nodes, sizeof(tlfr::QNode) * nn, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(ts.data(), c.node_tspan, sizeof(float2) * nn, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(p.data(), c.s_pos, sizeof(float4) * ns, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(m.data(), c.s_mot, sizeof(float4) * ns, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(col.data(), c.s_col, sizeof(float4) * ns, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(id.data(), c.s_id, sizeof(int) * ns, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "tree export: %s", cudaGetErrorString(e));
+    for (int i = 0; i < nn; i++)
+    {
+        const tlfr::QNode& n = q[i];
+        if (nodef)
+        {
+            float* f = nodef + (size_t)i * 14;
+            f[0] = n.a.x; f[1] = n.a.y; f[2] = n.a.z; f[3] = n.a.w;
+            f[4] = n.b.x; f[5] = n.b.y; f[6] = n.b.z; f[7] = n.b.w;
+            f[8] = n.c.x; f[9] = n.c.y; f[10] = n.c.z; f[11] = n.c.w;
+            f[12] = ts[i].x; f[13] = ts[i].y;
+        }
+        if (nodei)
+        {
+            int* d = nodei + (size_t)i * 5;
+            const bool leaf = n.d.x < 0;
+            d[0] = leaf ? -1 : n.d.x;
+            d[1] = leaf ? -1 : n.d.y;
+            d[2] = leaf ? n.d.z : -1;
+            d[3] = leaf ? n.d.w : -1;
+            d[4] = 0;
+        }
+    }
+    if (nodei)
+    {
+        // sample counts: leaves directly, internal nodes by a post-order pass from the root
+        std::vector<int> order;
+        order.reserve(nn);
+        std::vector<int> stack{ c.root };
+        while (!stack.empty())
+        {
+            int i = stack.back(); stack.pop_back();
+            order.push_back(i);
+            if (q[i].d.x >= 0) { stack.push_back(q[i].d.x); stack.push_back(q[i].d.y); }
+        }
+        for (auto it = order.rbegin(); it != order.rend(); ++it)
+        {
+            int i = *it;
+            int* d = nodei + (size_t)i * 5;
+            d[4] = (q[i].d.x < 0) ? (q[i].d.w - q[i].d.z) : (nodei[(size_t)q[i].d.x * 5 + 4] + nodei[(size_t)q[i].d.y * 5 + 4]);
+        }
+    }
+    for (int j = 0; j < ns; j++)
+    {
+        if (samplef)
+        {
+            float* f = samplef + (size_t)j * 12;
+            f[0] = p[j].x; f[1] = p[j].y; f[2] = p[j].z; f[3] = p[j].w;
+            f[4] = m[j].x; f[5] = m[j].y; f[6] = m[j].z;
+            f[7] = col[j].x; f[8] = col[j].y; f[9] = col[j].z; f[10] = col[j].w;
+            f[11] = p[j].z;     // key = w after reprojection (Reconstruction.hpp:119)
+        }
+        if (sample_ids) sample_ids[j] = id[j];
+    }
+    return TLFR_OK;
+}
+
+int tlfr_output_samples(tlfr_ctx* ctx, float* out5)
+{
+    if (!ctx)
+        return -1;
+    if (out5)
+        memcpy(out5, ctx->c.h_pattern.data(), sizeof(float) * ctx->c.h_pattern.size());
+    return (int)(ctx->c.h_pattern.size() / 5);
+}
+
+tlfr_status tlfr_trace_queries(tlfr_ctx* ctx, const int* xyi, int n, float* rgba, int* trace, int stride)
+{
+    if (!ctx || (n > 0 && (!xyi || !rgba || !trace || stride < 2)))
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_trace_queries: bad argument");
+    tlfr::Ctx& c = ctx->c;
+    cudaSetDevice(c.device);
+    for (int k = 0; k < n; k++)
+        if (xyi[3 * k] < 0 || xyi[3 * k] >= c.W || xyi[3 * k + 1] < 0 || xyi[3 * k + 1] >= c.H ||
+            xyi[3 * k + 2] < 0 || xyi[3 * k + 2] >= c.out_spp)
+            return fail(ctx, TLFR_BAD_ARG, "tlfr_trace_queries: query %d out of range", k);
+    return tlfr::trace_queries(c, xyi, n, rgba, trace, stride);
+}
+
+} // extern "C"

@@ -1,0 +1,178 @@
+// tlfr_internal.h — device data layout and the context shared by the build,
+// query and API translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "tlfr.h"
+#include "tlfr_common.cuh"
+
+namespace tlfr
+{
+
+// Hierarchy node as the query reads it: 64 bytes, one aligned 64-byte load.
+//   a = (xmin.t, xmin.uv, xmin.c, xmax.t)
+//   b = (xmax.uv, xmax.c, ymin.t, ymin.uv)
+//   c = (ymin.c, ymax.t, ymax.uv, ymax.c)
+//   d = (child0 or -1 for a leaf, child1, s0, s1)
+// Internal nodes' children are emitted as a pair, so child1 == child0 + 1.
+struct __align__(16) QNode
+{
+    float4 a, b, c;
+    int4   d;
+};
+
+// Node while the hierarchy is being built (Reconstruction.hpp:179-231 Node):
+// bounds, sample count, and either the sample range (leaf) or the emitted
+// children (internal).  80 bytes.
+struct __align__(16) BNode
+{
+    float p[12];        // planes xmin, xmax, ymin, ymax as (t, uv, const)
+    float tspan[2];
+    int   ref;          // >= 0: child0 slot of an internal node; < 0: leaf with s0 = ~ref
+    int   ns;
+    int   height;       // longest path to a leaf below, 1 for a leaf
+    int   pad;
+};
+
+// kd split of the reprojection grid (Reconstruction.hpp:169-177 InitialNode)
+struct __align__(16) KdNode
+{
+    int x0, y0, x1, y1;
+    int child0, child1;     // -1 for a leaf
+    int num_samples;        // samples in the subtree
+    int depth;
+    int path;               // child choices at depths 0..4 (bit j = depth j), i.e. the build task
+    int parent;
+    int leaf_count;         // kd leaves in the subtree
+    int preorder_leaf;      // preorder rank of the first kd leaf of the subtree
+    int preorder_sample;    // sample offset of the subtree in preorder
+    int sample_offset;      // final sample offset (task order, as the reference lays samples out)
+    int frontier;           // size of the subtree's frontier after emitNodes
+    int pad;
+};
+
+// Scalars computed on the device during the build.
+struct GridInfo
+{
+    float bbmin[2], bbmax[2];   // reprojected bounding box (before scaling)
+    int   max_hits;
+    int   num_valid;            // samples kept by the reprojection (w > 0)
+    float scale;
+    int   bmin_x, bmin_y;       // integer grid origin
+    int   gw, gh;               // grid size
+    int   num_kd;               // kd nodes
+    int   num_kd_leaves;
+    int   num_accepted;         // samples bucketed into the grid
+    int   num_nodes;            // emitted hierarchy nodes
+    int   root;
+    int   height;
+    int   entry[32];            // build task entry points (kd node or -1)
+    int   task_sample_base[32];
+    int   task_leaf_base[33];
+    int   num_invalid;          // samples with invalid bounds
+    int   error;                // nonzero: build capacity error code
+    int   kd_levels;
+};
+
+// Per-reconstruction device counters (TreeGather::Stats, Reconstruction.hpp:134-147).
+struct DevStats
+{
+    unsigned long long leaf_nodes, samples_in_leaves, within_1r, fetched, surfaces,
+                       num_2r, merged, at_least_one, overflow, empty;
+};
+
+struct Ctx
+{
+    // configuration
+    int W = 0, H = 0, spp_in = 0, spp = 1;
+    float coc0_raw[2] = { 0, 0 };   // header coefficients: drive the reprojection (Reconstruction.cpp:519)
+    float coc[2] = { 0, 0 };        // refocused coefficients (Reconstruction.cpp:77-87)
+    tlfr_params params{};
+    int out_spp = 128;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+
+    size_t n_in = 0;                // input records
+
+    // device buffers owned by the context
+    float* d_records = nullptr;     // 16-float records (owned copy when created from host)
+    bool   own_records = false;
+
+    // reprojected samples in input order
+    float4* rp_pos = nullptr;       // x, y, w, t
+    float4* rp_mot = nullptr;       // mv (3), valid flag
+    int*    rp_cell = nullptr;
+    int*    hits = nullptr;         // W*H
+    GridInfo* d_grid = nullptr;
+    GridInfo  grid{};               // host copy
+
+    // grid buckets
+    int* cell_count = nullptr;      // gw*gh (+1)
+    int* cell_start = nullptr;
+    int* cell_items = nullptr;      // input indices, bucketed
+    size_t cell_cap = 0;
+
+    // kd tree
+    KdNode* kd = nullptr;
+    int*    kd_level = nullptr;     // level ranges: [2*L], [2*L+1]
+    int*    kd_leaves_ordered = nullptr;   // kd leaf ids in build-task order
+    size_t  kd_cap = 0;
+
+    // per-sample build scratch (indexed by final sample slot)
+    int*    perm = nullptr;         // input index per slot (sorted candidates)
+    float*  box = nullptr;          // 8 floats per slot: boxa, boxb, boxaT1, boxbT1
+    Bounds* sbounds = nullptr;      // per-sample bounds
+    int*    surface = nullptr;      // surface id per slot
+    BNode*  pending = nullptr;      // frontier storage (indexed by slot)
+    int*    leaf_task_rank = nullptr;
+    int*    ordered_n = nullptr;    // candidate count per ordered leaf
+    int*    ordered_prefmax = nullptr;
+    BNode*  top = nullptr;          // serial-top scratch
+    size_t  samp_cap = 0;
+    size_t  leaf_cap = 0;
+
+    // final hierarchy
+    QNode*  nodes = nullptr;
+    float2* node_tspan = nullptr;   // time span per node (tree export only)
+    size_t  node_cap = 0;
+    float4* s_pos = nullptr;        // x, y, w, t  (tree order)
+    float4* s_mot = nullptr;        // mv (3), coc radius at w
+    float4* s_col = nullptr;        // rgba
+    int*    s_id = nullptr;         // input record index
+    int     num_samples = 0;
+    int     num_nodes = 0;
+    int     root = 0;
+    int     height = 0;
+
+    // output sampling pattern (64 * out_spp entries of x, y, u, v, t)
+    float*  d_pattern = nullptr;
+    std::vector<float> h_pattern;
+
+    // reconstruction
+    float4* accum = nullptr;        // per-pixel sums
+    int*    ovf_queue = nullptr;    // overflowing query ids
+    int*    ovf_count = nullptr;
+    size_t  ovf_cap = 0;
+    float*  ovf_scratch = nullptr;  // large-capacity per-query storage
+    size_t  ovf_scratch_bytes = 0;
+    DevStats* d_stats = nullptr;
+    float4* d_out = nullptr;        // device output when the caller passes host memory
+
+    tlfr_stats last{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+};
+
+// build: reprojection, bucketing, kd split, leaf construction, emitNodes, top.
+tlfr_status build_hierarchy(Ctx& c, const float* d_records);
+// query: all output samples of the frame into rgba (device pointer).
+tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats);
+tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h_trace, int stride);
+// host-side output pattern (Reconstruction.cpp:452-512)
+void generate_output_pattern(int out_spp, bool override_uvt, const float* uvt, std::vector<float>& out5);
+
+const char* cuda_error_string(cudaError_t e);
+
+} // namespace tlfr

@@ -1,0 +1,806 @@
+// tlfr_query.cu — per-output-sample reconstruction on the GPU.
+//
+// One thread answers one output sample (x, y, u, v, t) with the reference's
+// Filterer (reconstruction/ReconstructionOur.cpp:50-511):
+//   collect(R)   traversal (DFS, child1 popped first), leaf sort by w at the
+//                output time (FW::sort), per-sample reprojection and R test, and
+//                surface separation with sameSurface (Reconstruction.hpp:457-525)
+//   fetch2R      2R refetch and up to three widenings (RO.cpp:94-121)
+//   merge        tiny-surface merging (RO.cpp:137-156)
+//   resolve      per surface front to back: nearest tracking, coverage by
+//                triangles with double-precision edge functions, tent filter
+//                (RO.cpp:165-304), nearest-sample fallback (RO.cpp:318-348)
+// Pixels are the sum of their output samples normalised by alpha, red when
+// nothing was found (Reconstruction.cpp:649-720).
+//
+// Per-query working sets live in thread-local arrays with fixed capacities.  A
+// query that outgrows them is queued and re-run by k_query_overflow with large
+// capacities carved from a global arena; a query that outgrows those too is
+// reported as TLFR_OVERFLOW.
+#include "tlfr_common.cuh"
+#include "tlfr_internal.h"
+
+#include <cstdio>
+#include <cstring>
+
+namespace tlfr
+{
+
+namespace
+{
+
+struct Leaf { int node; float key; };
+struct RSample { float x, y; int index; int rpos; };        // ReconSample (Reconstruction.hpp:124-132)
+struct Surf { int start, n; float minDist; int minIndex; int quad; };
+
+struct Store
+{
+    int*     stack;   int stack_cap;
+    Leaf*    leaves;  int leaf_cap;
+    RSample* rs;      int rs_cap;
+    Surf*    surf;    int surf_cap;
+};
+
+struct QParams
+{
+    const QNode*  nodes;
+    const float4* s_pos;
+    const float4* s_mot;
+    const float4* s_col;
+    const float*  pattern;      // 64 * M * 5
+    int   M, W, H, root;
+    float c0, c1;               // refocused CoC coefficients
+    float disp0;
+    int   lens_filter, time_filter;
+};
+
+struct QStats
+{
+    unsigned leaves, in_leaves, within1r, fetched, surfaces, two_r, merged, at_least_one, empty;
+};
+
+struct Query { float x, y, u, v, t; };
+
+enum { kQOk = 0, kQOverflow = 1 };
+
+struct LeafSort
+{
+    Leaf* l;
+    TLFR_HD int cmp(int a, int b) const { return (l[a].key < l[b].key) ? -1 : (l[a].key > l[b].key) ? 1 : 0; }
+    TLFR_HD void swap(int a, int b) { Leaf t = l[a]; l[a] = l[b]; l[b] = t; }
+};
+
+TLFR_HD void node_planes(const QNode& n, float (&p)[4][3])
+{
+    p[0][0] = n.a.x; p[0][1] = n.a.y; p[0][2] = n.a.z;
+    p[1][0] = n.a.w; p[1][1] = n.b.x; p[1][2] = n.b.y;
+    p[2][0] = n.b.z; p[2][1] = n.b.w; p[2][2] = n.c.x;
+    p[3][0] = n.c.y; p[3][1] = n.c.z; p[3][2] = n.c.w;
+}
+
+// sameSurface (Reconstruction.hpp:457-525)
+TLFR_HD bool same_surface(const QNode& n0, const QNode& n1, const float* uvtmin, const float* uvtmax)
+{
+    const float TH = 1 * 0.1f;
+    float a[4][3], b[4][3];
+    node_planes(n0, a);
+    node_planes(n1, b);
+    float tmid = 0.5f * (uvtmin[2] + uvtmax[2]);
+    bool bCoC =
+        ternary_equal2(ternary_compare(plane_eval(a[0], tmid, uvtmin[0]), plane_eval(b[0], tmid, uvtmin[0]), TH),
+                       ternary_compare(plane_eval(a[0], tmid, uvtmax[0]), plane_eval(b[0], tmid, uvtmax[0]), TH)) &&
+        ternary_equal2(ternary_compare(plane_eval(a[2], tmid, uvtmin[1]), plane_eval(b[2], tmid, uvtmin[1]), TH),
+                       ternary_compare(plane_eval(a[2], tmid, uvtmax[1]), plane_eval(b[2], tmid, uvtmax[1]), TH)) &&
+        ternary_equal2(ternary_compare(plane_eval(a[1], tmid, uvtmin[0]), plane_eval(b[1], tmid, uvtmin[0]), TH),
+                       ternary_compare(plane_eval(a[1], tmid, uvtmax[0]), plane_eval(b[1], tmid, uvtmax[0]), TH)) &&
+        ternary_equal2(ternary_compare(plane_eval(a[3], tmid, uvtmin[1]), plane_eval(b[3], tmid, uvtmin[1]), TH),
+                       ternary_compare(plane_eval(a[3], tmid, uvtmax[1]), plane_eval(b[3], tmid, uvtmax[1]), TH));
+    if (!bCoC)
+        return false;
+    const float ta = uvtmin[2], tb = uvtmax[2];
+    return ternary_equal2(ternary_compare(plane_eval(a[0], ta, 0.0f), plane_eval(b[0], ta, 0.0f), TH),
+                          ternary_compare(plane_eval(a[0], tb, 0.0f), plane_eval(b[0], tb, 0.0f), TH)) &&
+           ternary_equal2(ternary_compare(plane_eval(a[1], ta, 0.0f), plane_eval(b[1], ta, 0.0f), TH),
+                          ternary_compare(plane_eval(a[1], tb, 0.0f), plane_eval(b[1], tb, 0.0f), TH)) &&
+           ternary_equal2(ternary_compare(plane_eval(a[2], ta, 0.0f), plane_eval(b[2], ta, 0.0f), TH),
+                          ternary_compare(plane_eval(a[2], tb, 0.0f), plane_eval(b[2], tb, 0.0f), TH)) &&
+           ternary_equal2(ternary_compare(plane_eval(a[3], ta, 0.0f), plane_eval(b[3], ta, 0.0f), TH),
+                          ternary_compare(plane_eval(a[3], tb, 0.0f), plane_eval(b[3], tb, 0.0f), TH));
+}
+
+// Node::intersect (Reconstruction.hpp:204-216)
+TLFR_HD bool node_intersect(const QNode& n, const Query& o, float R)
+{
+    float mnx = ((o.t * n.a.x + n.a.y * o.u) + n.a.z) - R;
+    float mny = ((o.t * n.b.z + n.b.w * o.v) + n.c.x) - R;
+    float mxx = ((o.t * n.a.w + n.b.x * o.u) + n.b.y) + R;
+    float mxy = ((o.t * n.c.y + n.c.z * o.v) + n.c.w) + R;
+    return (o.x >= mnx && o.y >= mny && o.x <= mxx && o.y <= mxy);
+}
+
+// collectInputSamples2 (RO.cpp:361-511).  Returns the number of samples within
+// R, or -1 when a capacity was exceeded.
+TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& nsurf, QStats& st)
+{
+    int nleaves = 0, sp = 0;
+    S.stack[sp++] = P.root;
+    while (sp > 0)
+    {
+        const int ni = S.stack[--sp];
+        const QNode node = P.nodes[ni];
+        if (node_intersect(node, o, R))
+        {
+            if (node.d.x < 0)
+            {
+                if (nleaves == S.leaf_cap)
+                    return -1;
+                const int s0 = node.d.z;
+                const float4 sp0 = P.s_pos[s0];
+                const float mvw = P.s_mot[s0].z;
+                S.leaves[nleaves].node = ni;
+                S.leaves[nleaves].key = sp0.z + (o.t - sp0.w) * mvw;
+                nleaves++;
+            }
+            else
+            {
+                if (sp + 2 > S.stack_cap)
+                    return -1;
+                S.stack[sp++] = node.d.x;
+                S.stack[sp++] = node.d.y;
+            }
+        }
+    }
+    st.leaves += nleaves;
+    LeafSort ls{ S.leaves };
+    fw_sort(ls, 0, nleaves);
+
+    nsurf = 0;
+    int nrs = 0, total = 0, surfaceStart = 0;
+    const float RANGE = 1.0f / sqrtf(128.0f);
+    const float uvtmin[3] = { o.u - RANGE, o.v - RANGE, o.t - 0.5f * RANGE };
+    const float uvtmax[3] = { o.u + RANGE, o.v + RANGE, o.t + 0.5f * RANGE };
+    const float R2 = R * R;
+    for (int lidx = 0; lidx < nleaves; lidx++)
+    {
+        bool first = true;
+        const QNode node = P.nodes[S.leaves[lidx].node];
+        const int s0 = node.d.z, s1 = node.d.w;
+        st.in_leaves += (unsigned)(s1 - s0);
+        for (int i = s0; i < s1; i++)
+        {
+            const float4 sp4 = P.s_pos[i];     // x, y, w, t
+            const float4 sm = P.s_mot[i];      // mv, coc(w)
+            float x, y, w;
+            if (sm.x != 0.0f || sm.y != 0.0f || sm.z != 0.0f)
+            {
+                const float dt = o.t - sp4.w;
+                const float Px = sp4.x * sp4.z + sm.x * dt;
+                const float Py = sp4.y * sp4.z + sm.y * dt;
+                const float Pw = (1.0f * sp4.z) + sm.z * dt;
+                w = Pw;
+                const float cr = rcp(Pw);
+                const float coc = P.c0 / w + P.c1;
+                x = Px * cr + o.u * coc;
+                y = Py * cr + o.v * coc;
+            }
+            else
+            {
+                w = sp4.z;
+                x = sp4.x + o.u * sm.w;
+                y = sp4.y + o.v * sm.w;
+            }
+            const float dx = x - o.x, dy = y - o.y;
+            const float dist2 = dx * dx + dy * dy;
+            if (dist2 <= R2)
+            {
+                if (first)
+                {
+                    first = false;
+                    bool same = true;
+                    for (int j = surfaceStart; j < lidx && same; ++j)
+                        same = same_surface(node, P.nodes[S.leaves[j].node], uvtmin, uvtmax);
+                    if (!same || nsurf == 0)
+                    {
+                        surfaceStart = lidx;
+                        if (nsurf == S.surf_cap)
+                            return -1;
+                        Surf& sf = S.surf[nsurf++];
+                        sf.start = nrs; sf.n = 0; sf.minDist = kF32Max; sf.minIndex = -1; sf.quad = 0;
+                    }
+                }
+                if (nrs == S.rs_cap)
+                    return -1;
+                Surf& sf = S.surf[nsurf - 1];
+                RSample r;
+                r.x = x; r.y = y; r.index = i;
+                r.rpos = (dx >= 0 ? 1 : 4) | (dy >= 0 ? 2 : 8);
+                S.rs[nrs++] = r;
+                sf.n++;
+                sf.quad |= (1 << (r.rpos & 3));
+                const float dist = sqrtf(dist2);
+                if (dist < sf.minDist)
+                {
+                    sf.minDist = dist;
+                    sf.minIndex = sf.n - 1;
+                }
+                total++;
+            }
+        }
+    }
+    st.fetched += total;
+    return total;
+}
+
+TLFR_HD void reverse(RSample* a, int lo, int hi)    // [lo, hi)
+{
+    for (hi--; lo < hi; lo++, hi--) { RSample t = a[lo]; a[lo] = a[hi]; a[hi] = t; }
+}
+
+TLFR_HD float len2(float dx, float dy) { return sqrtf(dx * dx + dy * dy); }
+
+struct EdgeFn { double A, B, C; bool acceptEqual; };
+
+// EdgeFunction (reconstruction_lib/common/EdgeFunction.cpp:39-45, .hpp:45-47)
+TLFR_HD EdgeFn edge_make(double x0, double y0, double x1, double y1)
+{
+    EdgeFn e;
+    e.A = y0 - y1;
+    e.B = x1 - x0;
+    e.C = (-x0) * e.A - y0 * e.B;
+    e.acceptEqual = (e.A == 0.) ? (e.B > 0.) : (e.A > 0.);
+    return e;
+}
+TLFR_HD bool edge_test(const EdgeFn& e, double x, double y)
+{
+    float d = d2f_rn((x * e.A + y * e.B) + e.C);
+    return d > 0.f ? true : (d == 0.f && e.acceptEqual);
+}
+
+TLFR_HD float gaussian(float x, float stddev, float mean)
+{
+    float e = 2.718281828f;
+    return powf(e, -((x - mean) * (x - mean)) / (2.0f * (stddev * stddev)));
+}
+
+// Filterer::reconstruct (RO.cpp:50-359).  trace, when given, receives the
+// flags and the final surfaces (layout documented in tlfr.h).
+template <bool TRACE>
+TLFR_HD int reconstruct_query(const QParams& P, Store& S, const Query& o, QStats& st, float4& out,
+                                 int* trace, int trace_cap)
+{
+    float dispersion = P.disp0;
+    int nsurf = 0;
+    int flags = 0;
+    int n1 = collect(P, S, o, dispersion, nsurf, st);
+    if (n1 < 0) return kQOverflow;
+    const bool fetch2R = nsurf == 0 || (S.surf[0].quad != 0xF && nsurf > 1);
+    if (fetch2R)
+    {
+        flags |= 1;
+        int n2 = collect(P, S, o, dispersion * 2, nsurf, st);
+        if (n2 < 0) return kQOverflow;
+        if (n2 == 0)
+        {
+            flags |= 2;
+            st.at_least_one++;
+            int nN = n2;
+            for (int k = 0; k < 3 && !nN; k++)
+            {
+                dispersion *= 2.f;
+                nN = collect(P, S, o, dispersion * 2, nsurf, st);
+                if (nN < 0) return kQOverflow;
+            }
+        }
+    }
+    st.two_r += fetch2R ? 1 : 0;
+    st.within1r += n1;
+
+    // tiny-surface merging: dst.samples += src.samples (src appended after dst)
+    int numSurfaces = nsurf;
+    if (fetch2R)
+        for (int sidx = 0; sidx < nsurf - 1; sidx++)
+        {
+            Surf& src = S.surf[sidx];
+            if (src.n < 4)
+            {
+                Surf& dst = S.surf[sidx + 1];
+                // src occupies [src.start, src.start+src.n), dst follows it; rotate to dst ++ src
+                const int lo = src.start, mid = src.start + src.n, hi = dst.start + dst.n;
+                if (src.n > 0 && mid == dst.start)
+                {
+                    reverse(S.rs, lo, mid);
+                    reverse(S.rs, mid, hi);
+                    reverse(S.rs, lo, hi);
+                }
+                dst.start = lo;
+                dst.n = hi - lo;
+                src.n = 0;
+                if (src.minDist < dst.minDist)
+                {
+                    dst.minDist = src.minDist;
+                    dst.minIndex = src.minIndex;
+                }
+                numSurfaces--;
+            }
+        }
+    st.surfaces += numSurfaces;
+    if (numSurfaces != nsurf)
+    {
+        st.merged++;
+        flags |= 4;
+    }
+
+    bool found = false;
+    float4 res = make_float4(0, 0, 0, 0);
+    float nearestDist = kF32Max;
+    int nearS = -1, nearI = 1;
+    for (int sidx = 0; sidx < nsurf && !found; sidx++)
+    {
+        const Surf sf = S.surf[sidx];
+        const int n = sf.n;
+        if (n == 0)
+            continue;
+        const RSample* in = S.rs + sf.start;
+        if (sf.minDist < nearestDist)
+        {
+            nearestDist = sf.minDist;
+            nearS = sidx; nearI = sf.minIndex;
+        }
+        if (!fetch2R || sf.minDist < 0.f || sidx == nsurf - 1)
+            found = true;
+        if (n >= 200)
+            found = true;
+        for (int m = 0; m < n - 2 && !found; m++)
+            for (int k = m + 1; k < n - 1 && !found; k++)
+            {
+                const RSample r0 = in[m], r1 = in[k];
+                const int rp01 = r0.rpos | r1.rpos;
+                for (int l = k + 1; l < n && !found; l++)
+                {
+                    const RSample r2 = in[l];
+                    if ((rp01 | r2.rpos) != 15)
+                        continue;
+                    if (len2(r0.x - r1.x, r0.y - r1.y) > 2 * dispersion ||
+                        len2(r0.x - r2.x, r0.y - r2.y) > 2 * dispersion ||
+                        len2(r1.x - r2.x, r1.y - r2.y) > 2 * dispersion)
+                        continue;
+                    if (len2(r0.x - o.x, r0.y - o.y) > dispersion &&
+                        len2(r1.x - o.x, r1.y - o.y) > dispersion &&
+                        len2(r2.x - o.x, r2.y - o.y) > dispersion)
+                        continue;
+                    EdgeFn e0 = edge_make(r1.x, r1.y, r2.x, r2.y);
+                    EdgeFn e1 = edge_make(r2.x, r2.y, r0.x, r0.y);
+                    EdgeFn e2 = edge_make(r0.x, r0.y, r1.x, r1.y);
+                    bool p0 = edge_test(e0, o.x, o.y);
+                    bool p1 = edge_test(e1, o.x, o.y);
+                    bool p2 = edge_test(e2, o.x, o.y);
+                    found = (p0 && p1 && p2) || (!p0 && !p1 && !p2);
+                }
+            }
+        if (found)
+        {
+            res = make_float4(0, 0, 0, 0);
+            for (int k = 0; k < n; k++)
+            {
+                const RSample r = in[k];
+                const float dx = o.x - r.x, dy = o.y - r.y;
+                const float weight = 1 - len2(dx, dy) / dispersion;
+                if (weight <= 0)
+                    continue;
+                const float4 c = P.s_col[r.index];
+                res.x += c.x * weight;
+                res.y += c.y * weight;
+                res.z += c.z * weight;
+                res.w += c.w * weight;
+            }
+            const float oow = rcp(res.w);
+            res.x *= oow; res.y *= oow; res.z *= oow; res.w *= oow;
+            nearS = sidx; nearI = sf.minIndex;
+        }
+    }
+
+    if (TRACE && trace)
+    {
+        int tn = 0;
+        auto put = [&](int v) { if (tn < trace_cap) trace[tn] = v; tn++; };
+        put(flags);
+        put(nsurf);
+        for (int s = 0; s < nsurf; s++)
+        {
+            put(S.surf[s].n);
+            put(S.surf[s].minIndex);
+            for (int k = 0; k < S.surf[s].n; k++)
+                put(S.rs[S.surf[s].start + k].index);
+        }
+        if (tn > trace_cap && trace_cap > 1)
+            trace[1] = -1;
+    }
+
+    if (nearS == -1)
+    {
+        st.empty++;
+        out = make_float4(0, 0, 0, 0);
+        return kQOk;
+    }
+    if (res.w == 0)
+    {
+        const RSample na = S.rs[S.surf[nearS].start + nearI];
+        res = P.s_col[na.index];
+    }
+    if (P.lens_filter == 1)
+    {
+        float g = gaussian(o.u, 0.5f, 0) * gaussian(o.v, 0.5f, 0);
+        res.x *= g; res.y *= g; res.z *= g; res.w *= g;
+    }
+    if (P.time_filter == 1)
+    {
+        float g = gaussian(o.t, 0.25f, 0.5f);
+        res.x *= g; res.y *= g; res.z *= g; res.w *= g;
+    }
+    out = res;
+    return kQOk;
+}
+
+// output sample i of pixel (x, y) (Reconstruction.cpp:653, 692-693)
+TLFR_HD Query make_query(const QParams& P, int x, int y, int i)
+{
+    const int pattern = (int)(hash_bits((uint32_t)x, (uint32_t)y) % 64u);
+    const float* s = P.pattern + ((size_t)pattern * P.M + i) * 5;
+    Query q;
+    q.x = s[0] + (float)x;
+    q.y = s[1] + (float)y;
+    q.u = s[2];
+    q.v = s[3];
+    q.t = s[4];
+    return q;
+}
+
+__device__ __forceinline__ void add_stats(QStats& a, const QStats& b)
+{
+    a.leaves += b.leaves; a.in_leaves += b.in_leaves; a.within1r += b.within1r; a.fetched += b.fetched;
+    a.surfaces += b.surfaces; a.two_r += b.two_r; a.merged += b.merged; a.at_least_one += b.at_least_one;
+    a.empty += b.empty;
+}
+
+__device__ void flush_stats(const QStats& st, DevStats* ds)
+{
+    // block-level reduction then one atomic per counter
+    __shared__ unsigned long long red[9];
+    if (threadIdx.x < 9) red[threadIdx.x] = 0;
+    __syncthreads();
+    unsigned v[9] = { st.leaves, st.in_leaves, st.within1r, st.fetched, st.surfaces, st.two_r, st.merged,
+                      st.at_least_one, st.empty };
+    for (int k = 0; k < 9; k++)
+    {
+        unsigned long long x = v[k];
+        for (int o = 16; o > 0; o >>= 1)
+            x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0)
+            atomicAdd(&red[k], x);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        atomicAdd(&ds->leaf_nodes, red[0]);
+        atomicAdd(&ds->samples_in_leaves, red[1]);
+        atomicAdd(&ds->within_1r, red[2]);
+        atomicAdd(&ds->fetched, red[3]);
+        atomicAdd(&ds->surfaces, red[4]);
+        atomicAdd(&ds->num_2r, red[5]);
+        atomicAdd(&ds->merged, red[6]);
+        atomicAdd(&ds->at_least_one, red[7]);
+        atomicAdd(&ds->empty, red[8]);
+    }
+}
+
+constexpr int kBlock = 128;
+constexpr int kStackCap = 64, kLeafCap = 128, kRsCap = 256, kSurfCap = 32;
+
+// Main pass: one thread per output sample; query id q = pixel * M + i.
+template <bool STATS>
+__global__ void __launch_bounds__(kBlock)
+k_query(QParams P, long long num_queries, float4* __restrict__ accum, int* __restrict__ ovf_queue,
+        int* __restrict__ ovf_count, int ovf_cap, DevStats* ds)
+{
+    int stack[kStackCap];
+    Leaf leaves[kLeafCap];
+    RSample rs[kRsCap];
+    Surf surf[kSurfCap];
+    Store S{ stack, kStackCap, leaves, kLeafCap, rs, kRsCap, surf, kSurfCap };
+    __shared__ float4 col[kBlock];
+    __shared__ int ok[kBlock];
+    QStats st{};
+    for (long long base = (long long)blockIdx.x * kBlock; base < num_queries; base += (long long)gridDim.x * kBlock)
+    {
+        const long long q = base + threadIdx.x;
+        float4 c = make_float4(0, 0, 0, 0);
+        int good = 0;
+        if (q < num_queries)
+        {
+            const long long pix = q / P.M;
+            const int i = (int)(q - pix * P.M);
+            const int x = (int)(pix % P.W), y = (int)(pix / P.W);
+            const Query o = make_query(P, x, y, i);
+            QStats qs{};
+            int r = reconstruct_query<false>(P, S, o, qs, c, nullptr, 0);
+            if (r == kQOk)
+            {
+                good = 1;
+                if (STATS) add_stats(st, qs);
+            }
+            else
+            {
+                int slot = atomicAdd(ovf_count, 1);
+                if (slot < ovf_cap)
+                    ovf_queue[slot] = (int)q;   // q < 2^31 checked on the host
+            }
+        }
+        col[threadIdx.x] = c;
+        ok[threadIdx.x] = good;
+        __syncthreads();
+        // sum each pixel's samples in sample order (Reconstruction.cpp:667-714)
+        if (q < num_queries)
+        {
+            const long long pix = q / P.M;
+            const bool head = threadIdx.x == 0 || ((q - 1) / P.M) != pix;
+            if (head)
+            {
+                float4 s = make_float4(0, 0, 0, 0);
+                int any = 0;
+                for (int t = threadIdx.x; t < kBlock && base + t < num_queries && (base + t) / P.M == pix; t++)
+                {
+                    if (!ok[t]) continue;
+                    s.x += col[t].x; s.y += col[t].y; s.z += col[t].z; s.w += col[t].w;
+                    any = 1;
+                }
+                if (any)
+                {
+                    atomicAdd(&accum[pix].x, s.x);
+                    atomicAdd(&accum[pix].y, s.y);
+                    atomicAdd(&accum[pix].z, s.z);
+                    atomicAdd(&accum[pix].w, s.w);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (STATS)
+        flush_stats(st, ds);
+}
+
+// Large-capacity pass for queries that overflowed the main pass.  Each thread
+// slot owns a fixed region of the arena.
+__global__ void __launch_bounds__(64)
+k_query_overflow(QParams P, const int* __restrict__ queue, int count, float4* __restrict__ accum, char* arena,
+                 size_t slot_bytes, int num_slots, int stack_cap, int leaf_cap, int rs_cap, int surf_cap,
+                 int* hard_fail, DevStats* ds, int stats)
+{
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    QStats st{};
+    if (slot < num_slots)
+    {
+        char* base = arena + (size_t)slot * slot_bytes;
+        Store S;
+        S.stack = (int*)base;                      S.stack_cap = stack_cap;
+        S.leaves = (Leaf*)(S.stack + stack_cap);   S.leaf_cap = leaf_cap;
+        S.rs = (RSample*)(S.leaves + leaf_cap);    S.rs_cap = rs_cap;
+        S.surf = (Surf*)(S.rs + rs_cap);           S.surf_cap = surf_cap;
+        for (int k = slot; k < count; k += num_slots)
+        {
+            const long long q = queue[k];
+            const long long pix = q / P.M;
+            const int i = (int)(q - pix * P.M);
+            const int x = (int)(pix % P.W), y = (int)(pix / P.W);
+            const Query o = make_query(P, x, y, i);
+            float4 c;
+            QStats qs{};
+            int r = reconstruct_query<false>(P, S, o, qs, c, nullptr, 0);
+            if (r != kQOk)
+            {
+                atomicAdd(hard_fail, 1);
+                continue;
+            }
+            add_stats(st, qs);
+            atomicAdd(&accum[pix].x, c.x);
+            atomicAdd(&accum[pix].y, c.y);
+            atomicAdd(&accum[pix].z, c.z);
+            atomicAdd(&accum[pix].w, c.w);
+        }
+    }
+    if (stats)
+        flush_stats(st, ds);
+}
+
+// pixelColor * rcp(pixelColor.w), red when empty (Reconstruction.cpp:716-719)
+__global__ void k_normalize(const float4* __restrict__ accum, float4* __restrict__ out, long long n)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+    {
+        float4 c = accum[p];
+        if (c.w == 0)
+            c = make_float4(1, 0, 0, 1);
+        float r = rcp(c.w);
+        out[p] = make_float4(c.x * r, c.y * r, c.z * r, c.w * r);
+    }
+}
+
+// Traced queries (parity tests): one thread per listed query, large capacities.
+__global__ void k_query_trace(QParams P, const int* __restrict__ xyi, int n, float4* __restrict__ rgba,
+                              int* __restrict__ trace, int stride, char* arena, size_t slot_bytes, int stack_cap,
+                              int leaf_cap, int rs_cap, int surf_cap)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    char* base = arena + (size_t)k * slot_bytes;
+    Store S;
+    S.stack = (int*)base;                      S.stack_cap = stack_cap;
+    S.leaves = (Leaf*)(S.stack + stack_cap);   S.leaf_cap = leaf_cap;
+    S.rs = (RSample*)(S.leaves + leaf_cap);    S.rs_cap = rs_cap;
+    S.surf = (Surf*)(S.rs + rs_cap);           S.surf_cap = surf_cap;
+    QStats st{};
+    const Query o = make_query(P, xyi[3 * k], xyi[3 * k + 1], xyi[3 * k + 2]);
+    float4 c = make_float4(0, 0, 0, 0);
+    int* tr = trace + (size_t)k * stride;
+    int r = reconstruct_query<true>(P, S, o, st, c, tr, stride);
+    if (r != kQOk && stride > 1)
+        tr[1] = -1;
+    rgba[k] = c;
+}
+
+size_t slot_bytes_for(int stack_cap, int leaf_cap, int rs_cap, int surf_cap)
+{
+    size_t b = sizeof(int) * stack_cap + sizeof(Leaf) * leaf_cap + sizeof(RSample) * rs_cap + sizeof(Surf) * surf_cap;
+    return (b + 255) & ~(size_t)255;
+}
+
+QParams make_params(const Ctx& c)
+{
+    QParams P;
+    P.nodes = c.nodes;
+    P.s_pos = c.s_pos;
+    P.s_mot = c.s_mot;
+    P.s_col = c.s_col;
+    P.pattern = c.d_pattern;
+    P.M = c.out_spp;
+    P.W = c.W;
+    P.H = c.H;
+    P.root = c.root;
+    P.c0 = c.coc[0];
+    P.c1 = c.coc[1];
+    P.disp0 = dispersion_for_spp(c.spp);
+    P.lens_filter = c.params.lens_filter;
+    P.time_filter = c.params.time_filter;
+    return P;
+}
+
+// overflow pass capacities
+constexpr int kOvStack = 512, kOvLeaf = 16384, kOvRs = 65536, kOvSurf = 4096;
+constexpr int kOvSlots = 2048;
+
+} // namespace
+
+#define CKQ(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { c.error = std::string(#x) + ": " + cudaGetErrorString(_e); return (_e == cudaErrorMemoryAllocation) ? TLFR_OOM : TLFR_CUDA; } } while (0)
+
+tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
+{
+    cudaStream_t s = c.stream;
+    const long long npix = (long long)c.W * c.H;
+    const long long nq = npix * c.out_spp;
+    if (nq >= (1ll << 31))
+    {
+        c.error = "more than 2^31 output samples in one frame";
+        return TLFR_BAD_ARG;
+    }
+    if (!c.accum)
+    {
+        CKQ(cudaMalloc(&c.accum, sizeof(float4) * npix));
+        CKQ(cudaMalloc(&c.d_stats, sizeof(DevStats) + 4 * sizeof(int)));
+        c.ovf_cap = (size_t)1 << 22;
+        CKQ(cudaMalloc(&c.ovf_queue, sizeof(int) * c.ovf_cap));
+        c.ovf_count = reinterpret_cast<int*>(c.d_stats + 1);
+    }
+    QParams P = make_params(c);
+    CKQ(cudaMemsetAsync(c.accum, 0, sizeof(float4) * npix, s));
+    CKQ(cudaMemsetAsync(c.d_stats, 0, sizeof(DevStats) + 4 * sizeof(int), s));
+    const int blocks = (int)std::min<long long>((nq + kBlock - 1) / kBlock, 148LL * 64);
+    if (collect_stats)
+        k_query<true><<<blocks, kBlock, 0, s>>>(P, nq, c.accum, c.ovf_queue, c.ovf_count, (int)c.ovf_cap, c.d_stats);
+    else
+        k_query<false><<<blocks, kBlock, 0, s>>>(P, nq, c.accum, c.ovf_queue, c.ovf_count, (int)c.ovf_cap, c.d_stats);
+    CKQ(cudaGetLastError());
+    int novf = 0;
+    CKQ(cudaMemcpyAsync(&novf, c.ovf_count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CKQ(cudaStreamSynchronize(s));
+    if (novf > (int)c.ovf_cap)
+    {
+        c.error = "overflow queue capacity exceeded";
+        return TLFR_OVERFLOW;
+    }
+    int hard = 0;
+    if (novf > 0)
+    {
+        const size_t sb = slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf);
+        if (!c.ovf_scratch)
+        {
+            c.ovf_scratch_bytes = sb * kOvSlots;
+            CKQ(cudaMalloc(&c.ovf_scratch, c.ovf_scratch_bytes));
+        }
+        const int slots = std::min(kOvSlots, novf);
+        k_query_overflow<<<(slots + 63) / 64, 64, 0, s>>>(P, c.ovf_queue, novf, c.accum, (char*)c.ovf_scratch, sb,
+                                                          slots, kOvStack, kOvLeaf, kOvRs, kOvSurf,
+                                                          c.ovf_count + 1, c.d_stats, collect_stats ? 1 : 0);
+        CKQ(cudaGetLastError());
+        CKQ(cudaMemcpyAsync(&hard, c.ovf_count + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    }
+    k_normalize<<<(int)std::min<long long>((npix + 255) / 256, 148LL * 16), 256, 0, s>>>(c.accum, d_rgba, npix);
+    CKQ(cudaGetLastError());
+    if (collect_stats)
+    {
+        DevStats ds;
+        CKQ(cudaMemcpyAsync(&ds, c.d_stats, sizeof(ds), cudaMemcpyDeviceToHost, s));
+        CKQ(cudaStreamSynchronize(s));
+        c.last.num_output_samples = (double)nq;
+        c.last.num_leaf_nodes = (double)ds.leaf_nodes;
+        c.last.num_samples_in_leaf_nodes = (double)ds.samples_in_leaves;
+        c.last.num_samples_within_1r = (double)ds.within_1r;
+        c.last.num_samples_fetched = (double)ds.fetched;
+        c.last.num_surfaces = (double)ds.surfaces;
+        c.last.num_2r = (double)ds.num_2r;
+        c.last.num_surfaces_merged = (double)ds.merged;
+        c.last.num_at_least_one = (double)ds.at_least_one;
+        c.last.num_empty = (double)ds.empty;
+    }
+    c.last.num_overflow_queries = novf;
+    if (hard > 0)
+    {
+        c.error = "a query exceeded the largest supported capacity";
+        return TLFR_OVERFLOW;
+    }
+    return TLFR_OK;
+}
+
+tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h_trace, int stride)
+{
+    if (n <= 0)
+        return TLFR_OK;
+    cudaStream_t s = c.stream;
+    const int stack_cap = 1024, leaf_cap = 16384, rs_cap = 65536, surf_cap = 4096;
+    const size_t sb = slot_bytes_for(stack_cap, leaf_cap, rs_cap, surf_cap);
+    int* d_xyi = nullptr; float4* d_rgba = nullptr; int* d_trace = nullptr; char* arena = nullptr;
+    tlfr_status st = TLFR_OK;
+    const int chunk = 1024;
+    QParams P = make_params(c);
+    do
+    {
+        if (cudaMalloc(&d_xyi, sizeof(int) * 3 * chunk) != cudaSuccess ||
+            cudaMalloc(&d_rgba, sizeof(float4) * chunk) != cudaSuccess ||
+            cudaMalloc(&d_trace, sizeof(int) * (size_t)stride * chunk) != cudaSuccess ||
+            cudaMalloc(&arena, sb * chunk) != cudaSuccess)
+        {
+            c.error = "trace_queries: allocation failed";
+            st = TLFR_OOM;
+            break;
+        }
+        for (int b = 0; b < n; b += chunk)
+        {
+            int m = std::min(chunk, n - b);
+            cudaMemcpyAsync(d_xyi, h_xyi + 3 * b, sizeof(int) * 3 * m, cudaMemcpyHostToDevice, s);
+            k_query_trace<<<(m + 63) / 64, 64, 0, s>>>(P, d_xyi, m, d_rgba, d_trace, stride, arena, sb, stack_cap,
+                                                       leaf_cap, rs_cap, surf_cap);
+            cudaMemcpyAsync(h_rgba + 4 * (size_t)b, d_rgba, sizeof(float4) * m, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(h_trace + (size_t)stride * b, d_trace, sizeof(int) * (size_t)stride * m,
+                            cudaMemcpyDeviceToHost, s);
+        }
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+        {
+            c.error = std::string("trace_queries: ") + cudaGetErrorString(e);
+            st = TLFR_CUDA;
+        }
+    } while (0);
+    cudaFree(d_xyi); cudaFree(d_rgba); cudaFree(d_trace); cudaFree(arena);
+    return st;
+}
+
+} // namespace tlfr

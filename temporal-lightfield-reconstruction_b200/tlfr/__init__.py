@@ -1,0 +1,320 @@
+"""Python binding of libtlfr.so, the B200 temporal light field reconstruction library.
+
+Mirrors the reference reconstruction library's interface
+(reference src/reconstruction_lib):
+
+    UVTSampleBuffer(path)                     common/SampleBuffer.cpp:230-387
+    UVTSampleBuffer.serialize(...)            common/SampleBuffer.cpp:404-564
+    CameraParams                              common/CameraParams.hpp:74-107
+    TreeGather(sbuf, params, aperture, focus) reconstruction/Reconstruction.hpp:45
+    TreeGather.reconstructDofMotion(image)    reconstruction/Reconstruction.cpp:221-295
+
+The library computes on the GPU only.  Loading fails loudly when libtlfr.so is
+missing; calls fail with TlfrError (status + message) when there is no CUDA
+device.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libtlfr.so")
+
+STATUS = {
+    0: "TLFR_OK", 1: "TLFR_BAD_ARG", 2: "TLFR_IO", 3: "TLFR_FORMAT", 4: "TLFR_OOM",
+    5: "TLFR_CUDA", 6: "TLFR_OVERFLOW", 7: "TLFR_TIMEOUT", 8: "TLFR_NO_DEVICE", 9: "TLFR_EMPTY",
+}
+
+SCENE_PLANES, SCENE_CARDS, SCENE_CARDS_LARGE = 0, 1, 2
+LENS_BOX, LENS_GAUSSIAN = 0, 1
+TIME_BOX, TIME_GAUSSIAN = 0, 1
+
+
+class TlfrError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("aperture_adjust", ctypes.c_float),
+        ("focus_adjust", ctypes.c_float),
+        ("lens_filter", ctypes.c_int),
+        ("time_filter", ctypes.c_int),
+        ("override_uvt", ctypes.c_int),
+        ("uvt", ctypes.c_float * 3),
+        ("output_spp", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "num_output_samples", "num_leaf_nodes", "num_samples_in_leaf_nodes", "num_samples_within_1r",
+        "num_samples_fetched", "num_surfaces", "num_2r", "num_surfaces_merged", "num_at_least_one",
+        "num_overflow_queries", "num_empty", "build_ms", "query_ms")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+_lib = None
+_VP = ctypes.c_void_p
+_FP = ctypes.POINTER(ctypes.c_float)
+_IP = ctypes.POINTER(ctypes.c_int)
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libtlfr.so (built by __graft_entry__.build() or `make` in the package)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libtlfr.so not found at {path}; build it with `make -C {os.path.dirname(path)}`")
+    lib = ctypes.CDLL(path)
+    sig = {
+        "tlfr_params_default": (None, [ctypes.POINTER(_Params)]),
+        "tlfr_buffer_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
+        "tlfr_buffer_from_host": (ctypes.c_int, [_FP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                                 ctypes.c_float, ctypes.POINTER(_VP)]),
+        "tlfr_buffer_save": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
+        "tlfr_buffer_info": (ctypes.c_int, [_VP, _IP, _IP, _IP, _FP, _FP]),
+        "tlfr_buffer_records": (_FP, [_VP]),
+        "tlfr_buffer_free": (None, [_VP]),
+        "tlfr_create": (ctypes.c_int, [_VP, ctypes.POINTER(_Params), _VP, ctypes.POINTER(_VP)]),
+        "tlfr_create_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                              ctypes.c_float, ctypes.POINTER(_Params), _VP, ctypes.POINTER(_VP)]),
+        "tlfr_rebuild_device": (ctypes.c_int, [_VP, _VP]),
+        "tlfr_reconstruct": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.POINTER(Stats)]),
+        "tlfr_set_output": (ctypes.c_int, [_VP, ctypes.POINTER(_Params)]),
+        "tlfr_sync": (ctypes.c_int, [_VP]),
+        "tlfr_get_stats": (ctypes.c_int, [_VP, ctypes.POINTER(Stats)]),
+        "tlfr_destroy": (None, [_VP]),
+        "tlfr_last_error": (ctypes.c_char_p, [_VP]),
+        "tlfr_tree_info": (ctypes.c_int, [_VP, _IP, _IP, _IP, _IP]),
+        "tlfr_tree_export": (ctypes.c_int, [_VP, _FP, _IP, _FP, _IP]),
+        "tlfr_output_samples": (ctypes.c_int, [_VP, _FP]),
+        "tlfr_trace_queries": (ctypes.c_int, [_VP, _IP, ctypes.c_int, _FP, _IP, ctypes.c_int]),
+        "tlfr_synth_scene": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_ulonglong, _FP, _FP]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _f32p(a: np.ndarray):
+    return a.ctypes.data_as(_FP)
+
+
+def _i32p(a: np.ndarray):
+    return a.ctypes.data_as(_IP)
+
+
+def _check(status: int, ctx=None):
+    if status != 0:
+        msg = load_library().tlfr_last_error(ctx)
+        raise TlfrError(status, msg.decode() if msg else "")
+
+
+def synth_scene(preset: int, width: int, height: int, spp: int, seed: int = 1):
+    """Seeded analytic scene -> (records float32 [H, W, spp, 16], (C0, C1))."""
+    lib = load_library()
+    rec = np.empty((height, width, spp, 16), np.float32)
+    coc = np.zeros(2, np.float32)
+    _check(lib.tlfr_synth_scene(preset, width, height, spp, seed, _f32p(rec), _f32p(coc)))
+    return rec, (float(coc[0]), float(coc[1]))
+
+
+class UVTSampleBuffer:
+    """Host sample buffer: W*H*spp records of 16 floats (SampleBuffer.cpp:283-286)."""
+
+    def __init__(self, path: Optional[str] = None, *, records=None, coc=None, width=None, height=None, spp=None):
+        lib = load_library()
+        h = _VP()
+        if path is not None:
+            _check(lib.tlfr_buffer_load(os.fsencode(path), ctypes.byref(h)))
+        else:
+            rec = np.ascontiguousarray(records, dtype=np.float32)
+            if width is None:
+                height, width, spp = rec.shape[:3]
+            _check(lib.tlfr_buffer_from_host(_f32p(rec), width, height, spp, coc[0], coc[1], ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        W, H, S = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        c0, c1 = ctypes.c_float(), ctypes.c_float()
+        _check(load_library().tlfr_buffer_info(self._h, ctypes.byref(W), ctypes.byref(H), ctypes.byref(S),
+                                               ctypes.byref(c0), ctypes.byref(c1)))
+        return W.value, H.value, S.value, (c0.value, c1.value)
+
+    def getWidth(self):
+        return self.info()[0]
+
+    def getHeight(self):
+        return self.info()[1]
+
+    def getCocCoeffs(self):
+        return self.info()[3]
+
+    def records(self) -> np.ndarray:
+        W, H, S, _ = self.info()
+        p = load_library().tlfr_buffer_records(self._h)
+        return np.ctypeslib.as_array(p, shape=(H, W, S, 16)).copy()
+
+    def serialize(self, path: str, separate_header: bool = False, binary: bool = False):
+        _check(load_library().tlfr_buffer_save(self._h, os.fsencode(path), int(separate_header), int(binary)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tlfr_buffer_free(self._h)
+            self._h = None
+
+
+@dataclass
+class CameraParams:
+    """The CameraParams fields the reconstruction path reads (CameraParams.hpp:74-107).
+
+    enableCuda selects the reference's CPU/GPU toggle; this library only has the
+    GPU side, so it must stay True.  overrideUVT: None or (u, v, t); the t=1
+    pinhole image is (0, 0, 1) (reconstruction_app/App.cpp:450).
+    """
+    lensFilter: int = LENS_BOX
+    timeFilter: int = TIME_BOX
+    overrideUVT: Optional[Tuple[float, float, float]] = None
+    enableCuda: bool = True
+    outputSpp: int = 0          # 0: reference default (128, or 1 with overrideUVT)
+    device: int = 0
+
+    def _to_c(self, aperture: float, focus: float) -> _Params:
+        if not self.enableCuda:
+            raise ValueError("enableCuda=False selects the CPU reconstruction, which this library does not provide")
+        p = _Params()
+        load_library().tlfr_params_default(ctypes.byref(p))
+        p.aperture_adjust = aperture
+        p.focus_adjust = focus
+        p.lens_filter = self.lensFilter
+        p.time_filter = self.timeFilter
+        if self.overrideUVT is not None:
+            p.override_uvt = 1
+            p.uvt[0], p.uvt[1], p.uvt[2] = self.overrideUVT
+        p.output_spp = self.outputSpp
+        p.device = self.device
+        return p
+
+
+class TreeGather:
+    """Hierarchy build + reconstruction (reconstruction/Reconstruction.hpp:42-48)."""
+
+    def __init__(self, sbuf: Optional[UVTSampleBuffer], params: Optional[CameraParams] = None,
+                 apertureAdjust: float = 1.0, focalDistanceAdjust: float = 1.0, *, stream: int = 0,
+                 device_records=None):
+        lib = load_library()
+        self.params = params or CameraParams()
+        p = self.params._to_c(apertureAdjust, focalDistanceAdjust)
+        h = _VP()
+        if device_records is not None:
+            ptr, (W, H, S), (c0, c1) = device_records
+            _check(lib.tlfr_create_device(_VP(ptr), W, H, S, c0, c1, ctypes.byref(p), _VP(stream), ctypes.byref(h)))
+            self.size = (W, H)
+        else:
+            _check(lib.tlfr_create(sbuf.handle, ctypes.byref(p), _VP(stream), ctypes.byref(h)))
+            self.size = sbuf.info()[:2]
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def reconstructDofMotion(self, image: Optional[np.ndarray] = None, stats: bool = False):
+        """RGBA float32 image [H, W, 4]; with stats=True returns (image, Stats)."""
+        W, H = self.size
+        if image is None:
+            image = np.empty((H, W, 4), np.float32)
+        st = Stats()
+        _check(load_library().tlfr_reconstruct(self._h, image.ctypes.data, 0, ctypes.byref(st) if stats else None),
+               self._h)
+        return (image, st) if stats else image
+
+    def reconstruct_to_device(self, dev_ptr: int, stats: bool = False):
+        st = Stats()
+        _check(load_library().tlfr_reconstruct(self._h, _VP(dev_ptr), 1, ctypes.byref(st) if stats else None),
+               self._h)
+        return st if stats else None
+
+    def rebuild(self, dev_ptr: int):
+        _check(load_library().tlfr_rebuild_device(self._h, _VP(dev_ptr)), self._h)
+
+    def set_output(self, params: CameraParams):
+        p = params._to_c(1.0, 1.0)
+        _check(load_library().tlfr_set_output(self._h, ctypes.byref(p)), self._h)
+        self.params = params
+
+    def stats(self) -> Stats:
+        st = Stats()
+        _check(load_library().tlfr_get_stats(self._h, ctypes.byref(st)), self._h)
+        return st
+
+    def tree_info(self):
+        n, s, r, h = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(load_library().tlfr_tree_info(self._h, ctypes.byref(n), ctypes.byref(s), ctypes.byref(r),
+                                             ctypes.byref(h)), self._h)
+        return n.value, s.value, r.value, h.value
+
+    def tree_export(self):
+        n, s, r, _ = self.tree_info()
+        nodef = np.zeros((n, 14), np.float32)
+        nodei = np.zeros((n, 5), np.int32)
+        samplef = np.zeros((s, 12), np.float32)
+        ids = np.zeros(s, np.int32)
+        _check(load_library().tlfr_tree_export(self._h, _f32p(nodef), _i32p(nodei), _f32p(samplef), _i32p(ids)),
+               self._h)
+        return nodef, nodei, samplef, ids, r
+
+    def output_samples(self) -> np.ndarray:
+        n = load_library().tlfr_output_samples(self._h, None)
+        out = np.zeros((n, 5), np.float32)
+        load_library().tlfr_output_samples(self._h, _f32p(out))
+        return out
+
+    def trace_queries(self, xyi: Sequence[Tuple[int, int, int]], stride: int = 4096):
+        q = np.ascontiguousarray(np.asarray(xyi, np.int32).reshape(-1, 3))
+        n = q.shape[0]
+        rgba = np.zeros((n, 4), np.float32)
+        trace = np.zeros((n, stride), np.int32)
+        _check(load_library().tlfr_trace_queries(self._h, _i32p(q), n, _f32p(rgba), _i32p(trace), stride), self._h)
+        return rgba, trace
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tlfr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def parse_trace(row: np.ndarray):
+    """Trace ints -> (flags, [(minIndex, [sample indices]), ...]); None if truncated."""
+    flags, ns = int(row[0]), int(row[1])
+    if ns < 0:
+        return None
+    k, surfaces = 2, []
+    for _ in range(ns):
+        n, mi = int(row[k]), int(row[k + 1])
+        surfaces.append((mi, [int(v) for v in row[k + 2:k + 2 + n]]))
+        k += 2 + n
+    return flags, surfaces
