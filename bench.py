@@ -1,0 +1,323 @@
+"""Benchmark: temporal light field reconstruction of one 1920x1080, 8 spp frame.
+
+Workload: 1920x1080 pixels, 8 input samples per pixel (16.6 M samples of 64 B),
+strong defocus (C0=-30, C1=40) and motion up to 60 px, 256 textured rectangles
++ 64 disks at depths log-uniform in [0.5, 100] (the seeded analytic scene
+TLFR_SCENE_CARDS_LARGE), 128 output samples per pixel (265 M output samples).
+
+A step is one full reconstruction of the frame from sample records resident in
+HBM: hierarchy build + per-output-sample query + pixel resolve.
+  value  Mpix/s over all ranks (W*H per rank per step / max-over-ranks step time)
+  e2e    the same through the public C ABI with host buffers: page-locked host
+         records -> device (tlfr_rebuild), build, reconstruct, RGBA image -> host
+  roofline   the query kernel's algorithmic bytes (64 B per leaf node tested,
+         32 B per sample tested, 16 B per sample accepted, summed over fetch
+         passes; + 16 B per output pixel) per launch / its CUDA-event duration,
+         against the measured HBM copy bandwidth.
+  cpu_baseline   the reference's own CPU reconstruction (oracle/_ref, or the C
+         restatement when the reference build is absent) on this host's cores:
+         full hierarchy build + a band of rows, extrapolated to the frame.
+
+Multi-GPU: one process per GPU, each reconstructs its own frame (replicas; the
+path has no exchange step), timed with CUDA events, max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "temporal-lightfield-reconstruction_b200")
+for p in (PKG, os.path.join(ROOT, "tests")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "recon Mpix/s on 1 B200: learned-routed vs plain GPU at <=0.1 dB loss; HBM GB/s"
+W, H, SPP, M = 1920, 1080, 8, 128
+PRESET = 2
+WORKLOAD = "1920x1080 8spp defocus+motion, 256 rects + 64 disks, 128 output samples/px"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-rows", type=int, default=8, help="rows per CPU baseline sample")
+    ap.add_argument("--width", type=int, default=W)
+    ap.add_argument("--height", type=int, default=H)
+    ap.add_argument("--spp", type=int, default=SPP)
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per query-kernel launch from the committed ncu summary, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "query_kernel_traffic.json")) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_sample(rec, coc, rows, threads):
+    """Reference CPU reconstruction timed on this host: full build + `rows` rows."""
+    from tlfr_testutil import CpuRecon, ref_available
+    kind = "reference" if ref_available() else "port"
+    os.environ["TLFR_REF_THREADS"] = str(threads)
+    r = CpuRecon("ref" if kind == "reference" else "orc", rec, coc, nthreads=threads)
+    Hh, Ww = rec.shape[0], rec.shape[1]
+    y0 = Hh // 2 - rows // 2
+    r.reconstruct_rows(y0, y0 + rows)
+    band = r.last_seconds
+    est = r.build_seconds + band * (Hh / rows)
+    r.close()
+    return {
+        "value": (Ww * Hh / est) / 1e6, "unit": "Mpix/s", "cores": threads, "kind": kind,
+        "sample": f"full {Ww}x{Hh} hierarchy build ({r.build_seconds:.2f} s) + rows [{y0},{y0 + rows}) of the query "
+                  f"({band:.2f} s), extrapolated to {Hh} rows",
+        "build_s": r.build_seconds, "band_s": band,
+    }
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU implementation on the host cores."""
+    if rank != 0:
+        return
+    import tlfr
+    from tlfr_testutil import CpuRecon, ref_available
+    threads = os.cpu_count() or 1
+    kind = "reference" if ref_available() else "port"
+    os.environ["TLFR_REF_THREADS"] = str(threads)
+    rec, coc = tlfr.synth_scene(PRESET, args.width, args.height, args.spp, 2)
+    r = CpuRecon("ref" if kind == "reference" else "orc", rec, coc, nthreads=threads)
+    rows = max(1, args.cpu_rows // 2)
+    vals = []
+    Hh = args.height
+    for k in range(args.warmup + args.steps):
+        y0 = (Hh // 2 + 37 * k) % (Hh - rows)
+        r.reconstruct_rows(y0, y0 + rows)
+        est = r.build_seconds + r.last_seconds * (Hh / rows)
+        if k >= args.warmup:
+            vals.append(est)
+    t = statistics.median(vals)
+    value = (args.width * Hh / t) / 1e6
+    sample = (f"full {args.width}x{Hh} hierarchy build ({r.build_seconds:.2f} s, once) + per step {rows} rows of the "
+              f"query, extrapolated to the frame")
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic scene)", "impl": "reference",
+        "config": {"workload": WORKLOAD, "width": args.width, "height": Hh, "spp": args.spp, "output_spp": M},
+        "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    import tlfr
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    Wd, Hd, S = args.width, args.height, args.spp
+    rec, coc = tlfr.synth_scene(PRESET, Wd, Hd, S, 2 + rank)
+    stream = torch.cuda.current_stream()
+    d_rec = torch.from_numpy(rec).cuda()
+    params = tlfr.CameraParams(device=local_rank)
+    tg = tlfr.TreeGather(None, params, stream=stream.cuda_stream,
+                         device_records=(d_rec.data_ptr(), (Wd, Hd, S), coc))
+    out = torch.empty((Hd, Wd, 4), dtype=torch.float32, device="cuda")
+
+    def step():
+        tg.rebuild(d_rec.data_ptr())
+        tg.reconstruct_to_device(out.data_ptr())
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+
+    # counters for the algorithmic-byte roofline (untimed run)
+    st = tg.reconstruct_to_device(out.data_ptr(), stats=True)
+    alg_bytes = 64.0 * st.num_leaf_nodes + 32.0 * st.num_samples_in_leaf_nodes + 16.0 * st.num_samples_fetched \
+        + 16.0 * Wd * Hd
+
+    # timed region: inputs (1 GB records, ~1 GB hierarchy) exceed the 126 MB L2
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    q_ms, b_ms, l_ms, h_ms, launches = [], [], [], [], 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        tg.rebuild(d_rec.data_ptr())
+        sb = tg.stats()
+        s2 = tg.reconstruct_to_device(out.data_ptr(), stats=False)
+        sq = tg.stats()
+        b_ms.append(sb.build_ms)
+        q_ms.append(sq.query_kernel_ms)
+        l_ms.append(sq.light_ms)
+        h_ms.append(sq.heavy_ms)
+        launches += int(sb.build_launches + sq.query_launches)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = (world * Wd * Hd * args.steps / (total_ms / 1e3)) / 1e6
+
+    # end to end through the public API with host buffers (pinned records in,
+    # RGBA image out); every rank runs it, timed by its own clock, max over ranks
+    buf = tlfr.UVTSampleBuffer(records=rec, coc=coc)
+    img = np.empty((Hd, Wd, 4), np.float32)
+    tg.rebuild_from(buf)
+    tg.reconstructDofMotion(img)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        tg.rebuild_from(buf)
+        tg.reconstructDofMotion(img)
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": (world * Wd * Hd / e2e_s) / 1e6, "unit": "Mpix/s", "ms_per_step": e2e_s * 1e3,
+           "h2d_bytes_per_step": int(rec.nbytes), "d2h_bytes_per_step": int(img.nbytes)}
+
+    peaks, peak_kind = measured_peaks()
+    q_mean = statistics.mean(q_ms)
+    achieved = alg_bytes / (q_mean / 1e3) / 1e9
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+        "frac": achieved / peaks["hbm_gbs"], "traffic": ncu_traffic(), "kernel": "k_query",
+        "peak_source": f"{peak_kind} HBM copy bandwidth", "algorithmic_bytes_per_launch": alg_bytes,
+        "query_kernel_ms": q_mean,
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic scene, records resident in HBM)",
+        "config": {"workload": WORKLOAD, "width": Wd, "height": Hd, "spp": S, "output_spp": M,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (1.06 GB records, ~1 GB hierarchy)"},
+        "build_ms": statistics.mean(b_ms), "query_kernel_ms": q_mean,
+        "light_pass_ms": statistics.mean(l_ms), "heavy_pass_ms": statistics.mean(h_ms),
+        "heavy_queries": sq.num_heavy_queries,
+        "recon_samples_per_s": world * Wd * Hd * M * args.steps / (total_ms / 1e3),
+        "query_stats": {"leaf_nodes_per_query": st.num_leaf_nodes / st.num_output_samples,
+                        "samples_tested_per_query": st.num_samples_in_leaf_nodes / st.num_output_samples,
+                        "samples_fetched_per_query": st.num_samples_fetched / st.num_output_samples,
+                        "frac_2r": st.num_2r / st.num_output_samples,
+                        "overflow_queries": st.num_overflow_queries},
+        "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(rec, coc, args.cpu_rows, os.cpu_count() or 1)
+    tg.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

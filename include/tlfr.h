@@ -90,6 +90,16 @@ typedef struct tlfr_stats
     double num_empty;                 /* output samples that found no sample at all        */
     double build_ms;                  /* device time of the last hierarchy build           */
     double query_ms;                  /* device time of the last reconstruction            */
+    double query_kernel_ms;           /* device time of the main query kernel alone        */
+    double build_launches;            /* kernels launched by the last hierarchy build      */
+    double query_launches;            /* kernels launched by the last reconstruction       */
+    double overflow_leaves;           /* queries that outgrew the main pass, by capacity:  */
+    double overflow_stack;            /*   leaf list, traversal stack, surface list,       */
+    double overflow_surfaces;         /*   accepted-sample list (counted when stats are    */
+    double overflow_samples;          /*   requested)                                      */
+    double num_heavy_queries;         /* output samples that needed the full (2R) path      */
+    double light_ms;                  /* device time of the light (1R) pass                 */
+    double heavy_ms;                  /* device time of the full-path pass                  */
 } tlfr_stats;
 
 /* ---- sample buffers ------------------------------------------------------- */
@@ -127,6 +137,12 @@ tlfr_status tlfr_create_device(const float* d_records16, int width, int height, 
 /* Rebuild the hierarchy of an existing context from new device records of the same
  * size, reusing its device memory (no allocation when the sizes still fit).       */
 tlfr_status tlfr_rebuild_device(tlfr_ctx* ctx, const float* d_records16);
+
+/* Same from a host buffer of the same size: the records are copied to the
+ * context's device memory on its stream, then the hierarchy is rebuilt.  Buffers
+ * made by tlfr_buffer_from_host / tlfr_buffer_load live in page-locked memory when
+ * a CUDA device is present, so the copy runs at full PCIe rate.                   */
+tlfr_status tlfr_rebuild(tlfr_ctx* ctx, const tlfr_buffer* buf);
 
 /* reconstructDofMotion: one RGBA float pixel per buffer pixel, row-major, alpha 1,
  * (1,0,0,1) where no sample was found (Reconstruction.cpp:716-719).

@@ -17,11 +17,37 @@
 #include <string>
 #include <vector>
 
+// Records live in page-locked memory when a CUDA device is present (full-rate
+// host-to-device copies), in ordinary memory otherwise.
 struct tlfr_buffer
 {
     int W = 0, H = 0, spp = 0;
     float coc[2] = { 0, 0 };
-    std::vector<float> rec;     // W*H*spp*16
+    float* rec = nullptr;       // W*H*spp*16
+    size_t n = 0;               // records
+    bool pinned = false;
+
+    bool alloc(size_t records)
+    {
+        n = records;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0 &&
+            cudaMallocHost((void**)&rec, sizeof(float) * 16 * (n ? n : 1)) == cudaSuccess)
+            pinned = true;
+        else
+        {
+            cudaGetLastError();
+            rec = (float*)malloc(sizeof(float) * 16 * (n ? n : 1));
+            pinned = false;
+        }
+        return rec != nullptr;
+    }
+    ~tlfr_buffer()
+    {
+        if (!rec) return;
+        if (pinned) cudaFreeHost(rec);
+        else        free(rec);
+    }
 };
 
 struct tlfr_ctx
@@ -328,13 +354,16 @@ void free_ctx_buffers(tlfr::Ctx& c)
     void* ptrs[] = { c.own_records ? c.d_records : nullptr, c.rp_pos, c.rp_mot, c.rp_cell, c.hits, c.d_grid,
                      c.cell_count, c.cell_start, c.cell_items, c.kd, c.kd_level, c.kd_leaves_ordered, c.perm, c.box,
                      c.sbounds, c.surface, c.pending, c.leaf_task_rank, c.ordered_n, c.ordered_prefmax, c.top,
-                     c.nodes, c.node_tspan, c.s_pos, c.s_mot, c.s_col, c.s_id, c.d_pattern, c.accum, c.ovf_queue,
+                     c.nodes, c.node_tspan, c.s_pos, c.s_mot, c.s_col, c.s_id, c.d_pattern, c.accum, c.qcol, c.heavy_queue, c.ovf_queue,
                      c.ovf_scratch, c.d_stats, c.d_out };
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.ev0) cudaEventDestroy(c.ev0);
     if (c.ev1) cudaEventDestroy(c.ev1);
     if (c.ev2) cudaEventDestroy(c.ev2);
+    if (c.evq0) cudaEventDestroy(c.evq0);
+    if (c.evq1) cudaEventDestroy(c.evq1);
+    if (c.evq2) cudaEventDestroy(c.evq2);
 }
 
 tlfr_status begin_ctx(const tlfr_params* params, void* stream, int W, int H, int spp, float c0, float c1,
@@ -393,7 +422,9 @@ tlfr_status run_build(tlfr_ctx* ctx, const float* d_rec)
 {
     tlfr::Ctx& c = ctx->c;
     cudaEventRecord(c.ev0, c.stream);
+    const long long l0 = c.launches;
     tlfr_status st = tlfr::build_hierarchy(c, d_rec);
+    c.last.build_launches = (double)(c.launches - l0);
     if (st != TLFR_OK)
         return st;
     cudaEventRecord(c.ev1, c.stream);
@@ -433,8 +464,8 @@ tlfr_status tlfr_buffer_from_host(const float* rec, int W, int H, int spp, float
     b->W = W; b->H = H; b->spp = spp;
     b->coc[0] = c0; b->coc[1] = c1;
     const size_t n = (size_t)W * H * spp;
-    try { b->rec.assign(rec, rec + n * 16); }
-    catch (...) { delete b; return fail(nullptr, TLFR_OOM, "host allocation failed"); }
+    if (!b->alloc(n)) { delete b; return fail(nullptr, TLFR_OOM, "host allocation failed"); }
+    memcpy(b->rec, rec, sizeof(float) * 16 * n);
     for (size_t k = 0; k < n; k++)
         b->rec[k * 16 + 10] = 1.0f;     // alpha forced to 1 (SampleBuffer.cpp:343, 372)
     *out = b;
@@ -489,11 +520,11 @@ tlfr_status tlfr_buffer_load(const char* path, tlfr_buffer** out)
     if (fscanf(fph, "%1023s\n", desc) != 1) {}
     b->W = W; b->H = H; b->spp = spp; b->coc[0] = c0; b->coc[1] = c1;
     const size_t n = (size_t)W * H * spp;
-    try { b->rec.assign(n * 16, 0.0f); }
-    catch (...) { cleanup(); delete b; return fail(nullptr, TLFR_OOM, "host allocation failed"); }
+    if (!b->alloc(n)) { cleanup(); delete b; return fail(nullptr, TLFR_OOM, "host allocation failed"); }
+    memset(b->rec, 0, sizeof(float) * 16 * n);
     if (binary)
     {
-        size_t got = fread(b->rec.data(), 64, n, fp);
+        size_t got = fread(b->rec, 64, n, fp);
         if (got != n)
         {
             cleanup(); delete b;
@@ -562,7 +593,7 @@ tlfr_status tlfr_buffer_save(const tlfr_buffer* b, const char* path, int separat
     bool ok = true;
     if (binary)
     {
-        std::vector<float> tmp(b->rec);
+        std::vector<float> tmp(b->rec, b->rec + 16 * n);
         for (size_t k = 0; k < n; k++)
             tmp[k * 16 + 10] = tmp[k * 16 + 9];
         ok = fwrite(tmp.data(), 64, n, fp) == n;
@@ -596,7 +627,7 @@ tlfr_status tlfr_buffer_info(const tlfr_buffer* b, int* W, int* H, int* spp, flo
     return TLFR_OK;
 }
 
-const float* tlfr_buffer_records(const tlfr_buffer* b) { return b ? b->rec.data() : nullptr; }
+const float* tlfr_buffer_records(const tlfr_buffer* b) { return b ? b->rec : nullptr; }
 void tlfr_buffer_free(tlfr_buffer* b) { delete b; }
 
 tlfr_status tlfr_create(const tlfr_buffer* buf, const tlfr_params* params, void* stream, tlfr_ctx** out)
@@ -615,7 +646,7 @@ tlfr_status tlfr_create(const tlfr_buffer* buf, const tlfr_params* params, void*
     if (e == cudaSuccess)
     {
         c.own_records = true;
-        e = cudaMemcpyAsync(c.d_records, buf->rec.data(), sizeof(float) * 16 * c.n_in, cudaMemcpyHostToDevice, c.stream);
+        e = cudaMemcpyAsync(c.d_records, buf->rec, sizeof(float) * 16 * c.n_in, cudaMemcpyHostToDevice, c.stream);
     }
     if (e != cudaSuccess)
     {
@@ -665,6 +696,29 @@ tlfr_status tlfr_rebuild_device(tlfr_ctx* ctx, const float* d_rec)
     return run_build(ctx, d_rec);
 }
 
+tlfr_status tlfr_rebuild(tlfr_ctx* ctx, const tlfr_buffer* buf)
+{
+    if (!ctx || !buf)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_rebuild: bad argument");
+    tlfr::Ctx& c = ctx->c;
+    if (buf->W != c.W || buf->H != c.H || buf->spp != c.spp_in || buf->coc[0] != c.coc0_raw[0] ||
+        buf->coc[1] != c.coc0_raw[1])
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_rebuild: buffer size or CoC coefficients differ from the context's");
+    cudaSetDevice(c.device);
+    cudaError_t e = cudaSuccess;
+    if (!c.d_records || !c.own_records)
+    {
+        e = cudaMalloc(&c.d_records, sizeof(float) * 16 * c.n_in);
+        if (e != cudaSuccess)
+            return fail(ctx, TLFR_OOM, "record allocation: %s", cudaGetErrorString(e));
+        c.own_records = true;
+    }
+    e = cudaMemcpyAsync(c.d_records, buf->rec, sizeof(float) * 16 * c.n_in, cudaMemcpyHostToDevice, c.stream);
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "record upload: %s", cudaGetErrorString(e));
+    return run_build(ctx, c.d_records);
+}
+
 tlfr_status tlfr_reconstruct(tlfr_ctx* ctx, float* rgba, int rgba_on_device, tlfr_stats* stats)
 {
     if (!ctx || !rgba)
@@ -684,7 +738,9 @@ tlfr_status tlfr_reconstruct(tlfr_ctx* ctx, float* rgba, int rgba_on_device, tlf
         dst = c.d_out;
     }
     cudaEventRecord(c.ev1, c.stream);
+    const long long l0 = c.launches;
     tlfr_status st = tlfr::reconstruct_frame(c, dst, stats != nullptr);
+    c.last.query_launches = (double)(c.launches - l0);
     cudaEventRecord(c.ev2, c.stream);
     if (st != TLFR_OK)
         return st;

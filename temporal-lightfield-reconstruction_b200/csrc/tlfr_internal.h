@@ -8,6 +8,10 @@
 #include "tlfr.h"
 #include "tlfr_common.cuh"
 
+// Kernel launch on the context's stream, counted in Ctx::launches.
+#define TLFR_LAUNCH(ctx, kern, grid, block, stream, ...) \
+    do { kern<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__); (ctx).launches++; } while (0)
+
 namespace tlfr
 {
 
@@ -81,6 +85,7 @@ struct DevStats
 {
     unsigned long long leaf_nodes, samples_in_leaves, within_1r, fetched, surfaces,
                        num_2r, merged, at_least_one, overflow, empty;
+    unsigned long long overflow_by_reason[4];   // [reason & 3]: 1 leaves, 2 stack, 3 surfaces, 0 samples
 };
 
 struct Ctx
@@ -152,7 +157,10 @@ struct Ctx
     std::vector<float> h_pattern;
 
     // reconstruction
-    float4* accum = nullptr;        // per-pixel sums
+    float4* qcol = nullptr;         // colour of every output sample of the frame
+    int*    heavy_queue = nullptr;  // output samples for the full path
+    size_t  qcol_cap = 0;
+    float4* accum = nullptr;        // unused
     int*    ovf_queue = nullptr;    // overflowing query ids
     int*    ovf_count = nullptr;
     size_t  ovf_cap = 0;
@@ -163,6 +171,8 @@ struct Ctx
 
     tlfr_stats last{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    cudaEvent_t evq0 = nullptr, evq1 = nullptr, evq2 = nullptr;   // around the query passes
+    long long launches = 0;                         // kernels launched by this context
 };
 
 // build: reprojection, bucketing, kd split, leaf construction, emitNodes, top.

@@ -57,6 +57,7 @@ struct QParams
 struct QStats
 {
     unsigned leaves, in_leaves, within1r, fetched, surfaces, two_r, merged, at_least_one, empty;
+    int overflow_reason;        // 0, or the capacity that was exceeded (1..4)
 };
 
 struct Query { float x, y, u, v, t; };
@@ -119,7 +120,8 @@ TLFR_HD bool node_intersect(const QNode& n, const Query& o, float R)
 }
 
 // collectInputSamples2 (RO.cpp:361-511).  Returns the number of samples within
-// R, or -1 when a capacity was exceeded.
+// R, or a negative code when a capacity was exceeded (-1 leaves, -2 stack,
+// -3 surfaces, -4 accepted samples).
 TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& nsurf, QStats& st)
 {
     int nleaves = 0, sp = 0;
@@ -133,7 +135,7 @@ TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& ns
             if (node.d.x < 0)
             {
                 if (nleaves == S.leaf_cap)
-                    return -1;
+                    return -1;   // leaf list full
                 const int s0 = node.d.z;
                 const float4 sp0 = P.s_pos[s0];
                 const float mvw = P.s_mot[s0].z;
@@ -144,7 +146,7 @@ TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& ns
             else
             {
                 if (sp + 2 > S.stack_cap)
-                    return -1;
+                    return -2;   // traversal stack full
                 S.stack[sp++] = node.d.x;
                 S.stack[sp++] = node.d.y;
             }
@@ -203,13 +205,13 @@ TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& ns
                     {
                         surfaceStart = lidx;
                         if (nsurf == S.surf_cap)
-                            return -1;
+                            return -3;   // surface list full
                         Surf& sf = S.surf[nsurf++];
                         sf.start = nrs; sf.n = 0; sf.minDist = kF32Max; sf.minIndex = -1; sf.quad = 0;
                     }
                 }
                 if (nrs == S.rs_cap)
-                    return -1;
+                    return -4;   // accepted-sample list full
                 Surf& sf = S.surf[nsurf - 1];
                 RSample r;
                 r.x = x; r.y = y; r.index = i;
@@ -272,13 +274,13 @@ TLFR_HD int reconstruct_query(const QParams& P, Store& S, const Query& o, QStats
     int nsurf = 0;
     int flags = 0;
     int n1 = collect(P, S, o, dispersion, nsurf, st);
-    if (n1 < 0) return kQOverflow;
+    if (n1 < 0) { st.overflow_reason = -n1; return kQOverflow; }
     const bool fetch2R = nsurf == 0 || (S.surf[0].quad != 0xF && nsurf > 1);
     if (fetch2R)
     {
         flags |= 1;
         int n2 = collect(P, S, o, dispersion * 2, nsurf, st);
-        if (n2 < 0) return kQOverflow;
+        if (n2 < 0) { st.overflow_reason = -n2; return kQOverflow; }
         if (n2 == 0)
         {
             flags |= 2;
@@ -288,7 +290,7 @@ TLFR_HD int reconstruct_query(const QParams& P, Store& S, const Query& o, QStats
             {
                 dispersion *= 2.f;
                 nN = collect(P, S, o, dispersion * 2, nsurf, st);
-                if (nN < 0) return kQOverflow;
+                if (nN < 0) { st.overflow_reason = -nN; return kQOverflow; }
             }
         }
     }
@@ -494,84 +496,269 @@ __device__ void flush_stats(const QStats& st, DevStats* ds)
 }
 
 constexpr int kBlock = 128;
-constexpr int kStackCap = 64, kLeafCap = 128, kRsCap = 256, kSurfCap = 32;
+// capacities of the full per-query path (statistics pass and heavy pass)
+constexpr int kStackCap = 96, kLeafCap = 256, kRsCap = 512, kSurfCap = 64;
+// capacities of the light pass
+constexpr int kLStack = 96, kLLeaf = 128;
 
-// Main pass: one thread per output sample; query id q = pixel * M + i.
-template <bool STATS>
+// Light pass (RO.cpp:94-99, 165-304 for the common case): the 1R fetch when it
+// settles the output sample by itself, i.e. when it ends with exactly one
+// surface, or when the first surface already holds samples in all four
+// quadrants by the time a second surface opens (fetch2R is false in both
+// cases, and the first surface is the resolved one).  The first surface's tent
+// filter is accumulated while its samples are accepted, in acceptance order,
+// which is the order the reference filters them in, so no per-sample list is
+// kept.  Returns 0 with the colour in out, or 1 when the output sample needs
+// the full path (2R fetch, or the leaf list outgrew its capacity).
+TLFR_HD int light_query(const QParams& P, int* stack, Leaf* leaves, const Query& o, float4& out)
+{
+    const float R = P.disp0;
+    int nleaves = 0, sp = 0;
+    stack[sp++] = P.root;
+    while (sp > 0)
+    {
+        const int ni = stack[--sp];
+        const QNode node = P.nodes[ni];
+        if (node_intersect(node, o, R))
+        {
+            if (node.d.x < 0)
+            {
+                if (nleaves == kLLeaf)
+                    return 1;
+                const int s0 = node.d.z;
+                const float4 sp0 = P.s_pos[s0];
+                const float mvw = P.s_mot[s0].z;
+                leaves[nleaves].node = ni;
+                leaves[nleaves].key = sp0.z + (o.t - sp0.w) * mvw;
+                nleaves++;
+            }
+            else
+            {
+                if (sp + 2 > kLStack)
+                    return 1;
+                stack[sp++] = node.d.x;
+                stack[sp++] = node.d.y;
+            }
+        }
+    }
+    LeafSort ls{ leaves };
+    fw_sort(ls, 0, nleaves);
+
+    const float RANGE = 1.0f / sqrtf(128.0f);
+    const float uvtmin[3] = { o.u - RANGE, o.v - RANGE, o.t - 0.5f * RANGE };
+    const float uvtmax[3] = { o.u + RANGE, o.v + RANGE, o.t + 0.5f * RANGE };
+    const float R2 = R * R;
+    int nsurf = 0, surfaceStart = 0, quad = 0, nearest = -1;
+    float minDist = kF32Max;
+    float4 acc = make_float4(0, 0, 0, 0);
+    for (int lidx = 0; lidx < nleaves; lidx++)
+    {
+        bool first = true;
+        const QNode node = P.nodes[leaves[lidx].node];
+        const int s0 = node.d.z, s1 = node.d.w;
+        for (int i = s0; i < s1; i++)
+        {
+            const float4 sp4 = P.s_pos[i];
+            const float4 sm = P.s_mot[i];
+            float x, y;
+            if (sm.x != 0.0f || sm.y != 0.0f || sm.z != 0.0f)
+            {
+                const float dt = o.t - sp4.w;
+                const float Px = sp4.x * sp4.z + sm.x * dt;
+                const float Py = sp4.y * sp4.z + sm.y * dt;
+                const float Pw = (1.0f * sp4.z) + sm.z * dt;
+                const float cr = rcp(Pw);
+                const float coc = P.c0 / Pw + P.c1;
+                x = Px * cr + o.u * coc;
+                y = Py * cr + o.v * coc;
+            }
+            else
+            {
+                x = sp4.x + o.u * sm.w;
+                y = sp4.y + o.v * sm.w;
+            }
+            const float dx = x - o.x, dy = y - o.y;
+            const float dist2 = dx * dx + dy * dy;
+            if (dist2 <= R2)
+            {
+                if (first)
+                {
+                    first = false;
+                    bool same = true;
+                    for (int j = surfaceStart; j < lidx && same; ++j)
+                        same = same_surface(node, P.nodes[leaves[j].node], uvtmin, uvtmax);
+                    if (!same || nsurf == 0)
+                    {
+                        if (nsurf == 1)
+                        {
+                            // a second surface opens: the first one is final
+                            if (quad == 0xF)
+                                goto resolved;
+                            return 1;
+                        }
+                        nsurf = 1;
+                        surfaceStart = lidx;
+                    }
+                }
+                quad |= 1 << (((dx >= 0 ? 1 : 4) | (dy >= 0 ? 2 : 8)) & 3);
+                const float dist = sqrtf(dist2);
+                if (dist < minDist)
+                {
+                    minDist = dist;
+                    nearest = i;
+                }
+                // tent filter over the first surface (RO.cpp:274-294); |o - r| == dist
+                const float weight = 1 - dist / R;
+                if (weight > 0)
+                {
+                    const float4 c = P.s_col[i];
+                    acc.x += c.x * weight;
+                    acc.y += c.y * weight;
+                    acc.z += c.z * weight;
+                    acc.w += c.w * weight;
+                }
+            }
+        }
+    }
+    if (nsurf == 0)
+        return 1;
+resolved:
+    {
+        const float oow = rcp(acc.w);
+        acc.x *= oow; acc.y *= oow; acc.z *= oow; acc.w *= oow;
+        if (acc.w == 0)
+            acc = P.s_col[nearest];
+        if (P.lens_filter == 1)
+        {
+            float g = gaussian(o.u, 0.5f, 0) * gaussian(o.v, 0.5f, 0);
+            acc.x *= g; acc.y *= g; acc.z *= g; acc.w *= g;
+        }
+        if (P.time_filter == 1)
+        {
+            float g = gaussian(o.t, 0.25f, 0.5f);
+            acc.x *= g; acc.y *= g; acc.z *= g; acc.w *= g;
+        }
+        out = acc;
+        return 0;
+    }
+}
+
+__device__ __forceinline__ Query query_of(const QParams& P, long long q)
+{
+    const long long pix = q / P.M;
+    const int i = (int)(q - pix * P.M);
+    return make_query(P, (int)(pix % P.W), (int)(pix / P.W), i);
+}
+
+// Append value to a queue when pred holds, one atomic per warp.  All 32 lanes
+// of the warp must call it.
+__device__ __forceinline__ void warp_append(int* queue, int* count, bool pred, int value)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m)
+        return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader)
+        base = atomicAdd(count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred)
+        queue[base + __popc(m & ((1u << lane) - 1))] = value;
+}
+
+// Pass 1: every output sample through the light path; the rest are queued.
+// Query id q = pixel * M + i.  The queue holds up to num_queries entries.
 __global__ void __launch_bounds__(kBlock)
-k_query(QParams P, long long num_queries, float4* __restrict__ accum, int* __restrict__ ovf_queue,
-        int* __restrict__ ovf_count, int ovf_cap, DevStats* ds)
+k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
+              int* __restrict__ heavy_count)
+{
+    int stack[kLStack];
+    Leaf leaves[kLLeaf];
+    for (long long base = (long long)blockIdx.x * kBlock; base < num_queries; base += (long long)gridDim.x * kBlock)
+    {
+        const long long q = base + threadIdx.x;
+        bool hv = false;
+        if (q < num_queries)
+        {
+            float4 c;
+            if (light_query(P, stack, leaves, query_of(P, q), c) == 0)
+                qcol[q] = c;
+            else
+                hv = true;
+        }
+        warp_append(heavy, heavy_count, hv, (int)q);
+    }
+}
+
+// Pass 2: the queued output samples through the full path (RO.cpp:50-359).
+// Samples that outgrow these capacities go to the large-capacity pass.
+__global__ void __launch_bounds__(kBlock)
+k_query_heavy(QParams P, const int* __restrict__ heavy, const int* __restrict__ heavy_count,
+              float4* __restrict__ qcol, int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap)
 {
     int stack[kStackCap];
     Leaf leaves[kLeafCap];
     RSample rs[kRsCap];
     Surf surf[kSurfCap];
     Store S{ stack, kStackCap, leaves, kLeafCap, rs, kRsCap, surf, kSurfCap };
-    __shared__ float4 col[kBlock];
-    __shared__ int ok[kBlock];
+    const int n = *heavy_count;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    {
+        const int q = heavy[k];
+        QStats qs{};
+        float4 c;
+        if (reconstruct_query<false>(P, S, query_of(P, q), qs, c, nullptr, 0) == kQOk)
+            qcol[q] = c;
+        else
+        {
+            int slot = atomicAdd(ovf_count, 1);
+            if (slot < ovf_cap)
+                ovf_queue[slot] = q;
+        }
+    }
+}
+
+// Statistics pass: every output sample through the full path with the
+// reference's counters (TreeGather::Stats).
+__global__ void __launch_bounds__(kBlock)
+k_query_stats(QParams P, long long num_queries, float4* __restrict__ qcol, int* __restrict__ ovf_queue,
+              int* __restrict__ ovf_count, int ovf_cap, DevStats* ds)
+{
+    int stack[kStackCap];
+    Leaf leaves[kLeafCap];
+    RSample rs[kRsCap];
+    Surf surf[kSurfCap];
+    Store S{ stack, kStackCap, leaves, kLeafCap, rs, kRsCap, surf, kSurfCap };
     QStats st{};
     for (long long base = (long long)blockIdx.x * kBlock; base < num_queries; base += (long long)gridDim.x * kBlock)
     {
         const long long q = base + threadIdx.x;
-        float4 c = make_float4(0, 0, 0, 0);
-        int good = 0;
         if (q < num_queries)
         {
-            const long long pix = q / P.M;
-            const int i = (int)(q - pix * P.M);
-            const int x = (int)(pix % P.W), y = (int)(pix / P.W);
-            const Query o = make_query(P, x, y, i);
             QStats qs{};
-            int r = reconstruct_query<false>(P, S, o, qs, c, nullptr, 0);
-            if (r == kQOk)
+            float4 c;
+            if (reconstruct_query<false>(P, S, query_of(P, q), qs, c, nullptr, 0) == kQOk)
             {
-                good = 1;
-                if (STATS) add_stats(st, qs);
+                qcol[q] = c;
+                add_stats(st, qs);
             }
             else
             {
+                atomicAdd(&ds->overflow_by_reason[qs.overflow_reason & 3], 1ull);
                 int slot = atomicAdd(ovf_count, 1);
                 if (slot < ovf_cap)
-                    ovf_queue[slot] = (int)q;   // q < 2^31 checked on the host
+                    ovf_queue[slot] = (int)q;
             }
         }
-        col[threadIdx.x] = c;
-        ok[threadIdx.x] = good;
-        __syncthreads();
-        // sum each pixel's samples in sample order (Reconstruction.cpp:667-714)
-        if (q < num_queries)
-        {
-            const long long pix = q / P.M;
-            const bool head = threadIdx.x == 0 || ((q - 1) / P.M) != pix;
-            if (head)
-            {
-                float4 s = make_float4(0, 0, 0, 0);
-                int any = 0;
-                for (int t = threadIdx.x; t < kBlock && base + t < num_queries && (base + t) / P.M == pix; t++)
-                {
-                    if (!ok[t]) continue;
-                    s.x += col[t].x; s.y += col[t].y; s.z += col[t].z; s.w += col[t].w;
-                    any = 1;
-                }
-                if (any)
-                {
-                    atomicAdd(&accum[pix].x, s.x);
-                    atomicAdd(&accum[pix].y, s.y);
-                    atomicAdd(&accum[pix].z, s.z);
-                    atomicAdd(&accum[pix].w, s.w);
-                }
-            }
-        }
-        __syncthreads();
     }
-    if (STATS)
-        flush_stats(st, ds);
+    flush_stats(st, ds);
 }
 
-// Large-capacity pass for queries that overflowed the main pass.  Each thread
-// slot owns a fixed region of the arena.
+// Pass 3: large capacities for queries that overflowed pass 2 (or the
+// statistics pass).  Each thread slot owns a fixed region of the arena.
 __global__ void __launch_bounds__(64)
-k_query_overflow(QParams P, const int* __restrict__ queue, int count, float4* __restrict__ accum, char* arena,
+k_query_overflow(QParams P, const int* __restrict__ queue, int count, float4* __restrict__ qcol, char* arena,
                  size_t slot_bytes, int num_slots, int stack_cap, int leaf_cap, int rs_cap, int surf_cap,
                  int* hard_fail, DevStats* ds, int stats)
 {
@@ -587,40 +774,40 @@ k_query_overflow(QParams P, const int* __restrict__ queue, int count, float4* __
         S.surf = (Surf*)(S.rs + rs_cap);           S.surf_cap = surf_cap;
         for (int k = slot; k < count; k += num_slots)
         {
-            const long long q = queue[k];
-            const long long pix = q / P.M;
-            const int i = (int)(q - pix * P.M);
-            const int x = (int)(pix % P.W), y = (int)(pix / P.W);
-            const Query o = make_query(P, x, y, i);
+            const int q = queue[k];
             float4 c;
             QStats qs{};
-            int r = reconstruct_query<false>(P, S, o, qs, c, nullptr, 0);
-            if (r != kQOk)
+            if (reconstruct_query<false>(P, S, query_of(P, q), qs, c, nullptr, 0) != kQOk)
             {
                 atomicAdd(hard_fail, 1);
+                qcol[q] = make_float4(0, 0, 0, 0);
                 continue;
             }
             add_stats(st, qs);
-            atomicAdd(&accum[pix].x, c.x);
-            atomicAdd(&accum[pix].y, c.y);
-            atomicAdd(&accum[pix].z, c.z);
-            atomicAdd(&accum[pix].w, c.w);
+            qcol[q] = c;
         }
     }
     if (stats)
         flush_stats(st, ds);
 }
 
-// pixelColor * rcp(pixelColor.w), red when empty (Reconstruction.cpp:716-719)
-__global__ void k_normalize(const float4* __restrict__ accum, float4* __restrict__ out, long long n)
+// Pixel = sum of its output samples in sample order, times rcp(alpha); red
+// when empty (Reconstruction.cpp:665-719).
+__global__ void k_resolve(const float4* __restrict__ qcol, int M, float4* __restrict__ out, long long npix)
 {
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x)
     {
-        float4 c = accum[p];
-        if (c.w == 0)
-            c = make_float4(1, 0, 0, 1);
-        float r = rcp(c.w);
-        out[p] = make_float4(c.x * r, c.y * r, c.z * r, c.w * r);
+        const float4* c = qcol + p * M;
+        float4 s = make_float4(0, 0, 0, 0);
+        for (int i = 0; i < M; i++)
+        {
+            const float4 v = c[i];
+            s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+        }
+        if (s.w == 0)
+            s = make_float4(1, 0, 0, 1);
+        const float r = rcp(s.w);
+        out[p] = make_float4(s.x * r, s.y * r, s.z * r, s.w * r);
     }
 }
 
@@ -676,7 +863,7 @@ QParams make_params(const Ctx& c)
 
 // overflow pass capacities
 constexpr int kOvStack = 512, kOvLeaf = 16384, kOvRs = 65536, kOvSurf = 4096;
-constexpr int kOvSlots = 2048;
+constexpr int kOvSlots = 4096;
 
 } // namespace
 
@@ -692,26 +879,51 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
         c.error = "more than 2^31 output samples in one frame";
         return TLFR_BAD_ARG;
     }
-    if (!c.accum)
+    if ((size_t)nq > c.qcol_cap)
     {
-        CKQ(cudaMalloc(&c.accum, sizeof(float4) * npix));
-        CKQ(cudaMalloc(&c.d_stats, sizeof(DevStats) + 4 * sizeof(int)));
+        cudaFree(c.qcol); cudaFree(c.heavy_queue);
+        c.qcol = nullptr; c.heavy_queue = nullptr; c.qcol_cap = 0;
+        CKQ(cudaMalloc(&c.qcol, sizeof(float4) * nq));
+        CKQ(cudaMalloc(&c.heavy_queue, sizeof(int) * nq));
+        c.qcol_cap = (size_t)nq;
+    }
+    if (!c.d_stats)
+    {
+        CKQ(cudaMalloc(&c.d_stats, sizeof(DevStats) + 8 * sizeof(int)));
         c.ovf_cap = (size_t)1 << 22;
         CKQ(cudaMalloc(&c.ovf_queue, sizeof(int) * c.ovf_cap));
-        c.ovf_count = reinterpret_cast<int*>(c.d_stats + 1);
     }
+    int* counters = reinterpret_cast<int*>(c.d_stats + 1);   // [0] overflow, [1] hard, [2] heavy
     QParams P = make_params(c);
-    CKQ(cudaMemsetAsync(c.accum, 0, sizeof(float4) * npix, s));
-    CKQ(cudaMemsetAsync(c.d_stats, 0, sizeof(DevStats) + 4 * sizeof(int), s));
+    CKQ(cudaMemsetAsync(c.d_stats, 0, sizeof(DevStats) + 8 * sizeof(int), s));
     const int blocks = (int)std::min<long long>((nq + kBlock - 1) / kBlock, 148LL * 64);
+    if (!c.evq0)
+    {
+        CKQ(cudaEventCreate(&c.evq0));
+        CKQ(cudaEventCreate(&c.evq1));
+        CKQ(cudaEventCreate(&c.evq2));
+    }
+    CKQ(cudaEventRecord(c.evq0, s));
     if (collect_stats)
-        k_query<true><<<blocks, kBlock, 0, s>>>(P, nq, c.accum, c.ovf_queue, c.ovf_count, (int)c.ovf_cap, c.d_stats);
+    {
+        TLFR_LAUNCH(c, k_query_stats, blocks, kBlock, s, P, nq, c.qcol, c.ovf_queue, counters + 0, (int)c.ovf_cap,
+                    c.d_stats);
+        CKQ(cudaEventRecord(c.evq1, s));
+    }
     else
-        k_query<false><<<blocks, kBlock, 0, s>>>(P, nq, c.accum, c.ovf_queue, c.ovf_count, (int)c.ovf_cap, c.d_stats);
+    {
+        TLFR_LAUNCH(c, k_query_light, blocks, kBlock, s, P, nq, c.qcol, c.heavy_queue, counters + 2);
+        CKQ(cudaEventRecord(c.evq1, s));
+        TLFR_LAUNCH(c, k_query_heavy, 148 * 16, kBlock, s, P, c.heavy_queue, counters + 2, c.qcol, c.ovf_queue,
+                    counters + 0, (int)c.ovf_cap);
+    }
+    CKQ(cudaEventRecord(c.evq2, s));
     CKQ(cudaGetLastError());
-    int novf = 0;
-    CKQ(cudaMemcpyAsync(&novf, c.ovf_count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    int host_counts[3] = { 0, 0, 0 };
+    CKQ(cudaMemcpyAsync(host_counts, counters, sizeof(int) * 3, cudaMemcpyDeviceToHost, s));
     CKQ(cudaStreamSynchronize(s));
+    const int novf = host_counts[0];
+    c.last.num_heavy_queries = host_counts[2];
     if (novf > (int)c.ovf_cap)
     {
         c.error = "overflow queue capacity exceeded";
@@ -727,29 +939,44 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
             CKQ(cudaMalloc(&c.ovf_scratch, c.ovf_scratch_bytes));
         }
         const int slots = std::min(kOvSlots, novf);
-        k_query_overflow<<<(slots + 63) / 64, 64, 0, s>>>(P, c.ovf_queue, novf, c.accum, (char*)c.ovf_scratch, sb,
-                                                          slots, kOvStack, kOvLeaf, kOvRs, kOvSurf,
-                                                          c.ovf_count + 1, c.d_stats, collect_stats ? 1 : 0);
+        TLFR_LAUNCH(c, k_query_overflow, (slots + 63) / 64, 64, s, P, c.ovf_queue, novf, c.qcol, (char*)c.ovf_scratch,
+                    sb, slots, kOvStack, kOvLeaf, kOvRs, kOvSurf, counters + 1, c.d_stats, collect_stats ? 1 : 0);
         CKQ(cudaGetLastError());
-        CKQ(cudaMemcpyAsync(&hard, c.ovf_count + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CKQ(cudaMemcpyAsync(&hard, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     }
-    k_normalize<<<(int)std::min<long long>((npix + 255) / 256, 148LL * 16), 256, 0, s>>>(c.accum, d_rgba, npix);
+    TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, 148LL * 32), 128, s, c.qcol, c.out_spp,
+                d_rgba, npix);
     CKQ(cudaGetLastError());
-    if (collect_stats)
+    {
+        float ms = 0, ms2 = 0;
+        CKQ(cudaEventElapsedTime(&ms, c.evq0, c.evq1));
+        CKQ(cudaEventElapsedTime(&ms2, c.evq1, c.evq2));
+        c.last.light_ms = ms;
+        c.last.heavy_ms = ms2;
+        c.last.query_kernel_ms = ms + ms2;
+    }
+    if (collect_stats || novf > 0)
     {
         DevStats ds;
         CKQ(cudaMemcpyAsync(&ds, c.d_stats, sizeof(ds), cudaMemcpyDeviceToHost, s));
         CKQ(cudaStreamSynchronize(s));
-        c.last.num_output_samples = (double)nq;
-        c.last.num_leaf_nodes = (double)ds.leaf_nodes;
-        c.last.num_samples_in_leaf_nodes = (double)ds.samples_in_leaves;
-        c.last.num_samples_within_1r = (double)ds.within_1r;
-        c.last.num_samples_fetched = (double)ds.fetched;
-        c.last.num_surfaces = (double)ds.surfaces;
-        c.last.num_2r = (double)ds.num_2r;
-        c.last.num_surfaces_merged = (double)ds.merged;
-        c.last.num_at_least_one = (double)ds.at_least_one;
-        c.last.num_empty = (double)ds.empty;
+        if (collect_stats)
+        {
+            c.last.num_output_samples = (double)nq;
+            c.last.num_leaf_nodes = (double)ds.leaf_nodes;
+            c.last.num_samples_in_leaf_nodes = (double)ds.samples_in_leaves;
+            c.last.num_samples_within_1r = (double)ds.within_1r;
+            c.last.num_samples_fetched = (double)ds.fetched;
+            c.last.num_surfaces = (double)ds.surfaces;
+            c.last.num_2r = (double)ds.num_2r;
+            c.last.num_surfaces_merged = (double)ds.merged;
+            c.last.num_at_least_one = (double)ds.at_least_one;
+            c.last.num_empty = (double)ds.empty;
+            c.last.overflow_leaves = (double)ds.overflow_by_reason[1];
+            c.last.overflow_stack = (double)ds.overflow_by_reason[2];
+            c.last.overflow_surfaces = (double)ds.overflow_by_reason[3];
+            c.last.overflow_samples = (double)ds.overflow_by_reason[0];
+        }
     }
     c.last.num_overflow_queries = novf;
     if (hard > 0)
@@ -786,7 +1013,7 @@ tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h
         {
             int m = std::min(chunk, n - b);
             cudaMemcpyAsync(d_xyi, h_xyi + 3 * b, sizeof(int) * 3 * m, cudaMemcpyHostToDevice, s);
-            k_query_trace<<<(m + 63) / 64, 64, 0, s>>>(P, d_xyi, m, d_rgba, d_trace, stride, arena, sb, stack_cap,
+            TLFR_LAUNCH(c, k_query_trace, (m + 63) / 64, 64, s, P, d_xyi, m, d_rgba, d_trace, stride, arena, sb, stack_cap,
                                                        leaf_cap, rs_cap, surf_cap);
             cudaMemcpyAsync(h_rgba + 4 * (size_t)b, d_rgba, sizeof(float4) * m, cudaMemcpyDeviceToHost, s);
             cudaMemcpyAsync(h_trace + (size_t)stride * b, d_trace, sizeof(int) * (size_t)stride * m,

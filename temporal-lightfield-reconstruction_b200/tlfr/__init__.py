@@ -58,7 +58,9 @@ class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "num_output_samples", "num_leaf_nodes", "num_samples_in_leaf_nodes", "num_samples_within_1r",
         "num_samples_fetched", "num_surfaces", "num_2r", "num_surfaces_merged", "num_at_least_one",
-        "num_overflow_queries", "num_empty", "build_ms", "query_ms")]
+        "num_overflow_queries", "num_empty", "build_ms", "query_ms", "query_kernel_ms", "build_launches",
+        "query_launches", "overflow_leaves", "overflow_stack", "overflow_surfaces", "overflow_samples",
+        "num_heavy_queries", "light_ms", "heavy_ms")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -91,6 +93,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_create_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                               ctypes.c_float, ctypes.POINTER(_Params), _VP, ctypes.POINTER(_VP)]),
         "tlfr_rebuild_device": (ctypes.c_int, [_VP, _VP]),
+        "tlfr_rebuild": (ctypes.c_int, [_VP, _VP]),
         "tlfr_reconstruct": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.POINTER(Stats)]),
         "tlfr_set_output": (ctypes.c_int, [_VP, ctypes.POINTER(_Params)]),
         "tlfr_sync": (ctypes.c_int, [_VP]),
@@ -256,7 +259,12 @@ class TreeGather:
         return st if stats else None
 
     def rebuild(self, dev_ptr: int):
+        """Rebuild the hierarchy from device records of the same size."""
         _check(load_library().tlfr_rebuild_device(self._h, _VP(dev_ptr)), self._h)
+
+    def rebuild_from(self, sbuf: "UVTSampleBuffer"):
+        """Upload a host buffer of the same size and rebuild the hierarchy."""
+        _check(load_library().tlfr_rebuild(self._h, sbuf.handle), self._h)
 
     def set_output(self, params: CameraParams):
         p = params._to_c(1.0, 1.0)
