@@ -189,6 +189,24 @@ int tlfr_output_samples(tlfr_ctx* ctx, float* out5);
 tlfr_status tlfr_trace_queries(tlfr_ctx* ctx, const int* xyi, int num_queries,
                                float* rgba, int* trace, int trace_stride);
 
+/* Allocation-free output-sample queries.  No counterpart in the reference: an
+ * addition for callers that cannot allocate device memory while they run (all
+ * memory reserved up front, an external allocator that owns the device heap, a
+ * thread that must not block on the allocator).  Same results as the colours of
+ * tlfr_trace_queries, for the output samples (x, y, i) in d_xyi[3*k ..] (device
+ * memory), written to d_rgba[4*k ..] (device memory).  The per-query working
+ * storage is a fixed 10.25 MiB device array inside the library (256 working
+ * slots), which every device that loads the library keeps until the process
+ * exits; nothing is allocated by the call.  A query that needs more than a slot
+ * holds (or an (x, y, i) out of range) yields (0, 0, 0, -1) and is counted in
+ * *d_overflow (device memory, may be NULL; set to zero by the call).
+ * num_queries <= 4194304 per call, else TLFR_BAD_ARG.  Asynchronous on the
+ * context's stream.  The first call on a device looks up the array's device
+ * address with that device current: make it before any stream capture.  All
+ * calls share the array, so calls whose work overlaps on the GPU race.       */
+tlfr_status tlfr_query_samples_noalloc(tlfr_ctx* ctx, const int* d_xyi, int num_queries, float* d_rgba,
+                                       int* d_overflow);
+
 /* ---- synthetic scenes (tests, benchmarks) ---------------------------------- */
 
 enum

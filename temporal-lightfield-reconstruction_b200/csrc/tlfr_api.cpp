@@ -904,6 +904,17 @@ int tlfr_output_samples(tlfr_ctx* ctx, float* out5)
     return (int)(ctx->c.h_pattern.size() / 5);
 }
 
+tlfr_status tlfr_query_samples_noalloc(tlfr_ctx* ctx, const int* d_xyi, int n, float* d_rgba, int* d_overflow)
+{
+    if (!ctx || (n > 0 && (!d_xyi || !d_rgba)))
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_query_samples_noalloc: bad argument");
+    tlfr::Ctx& c = ctx->c;
+    cudaError_t e = cudaSetDevice(c.device);
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "tlfr_query_samples_noalloc: %s", cudaGetErrorString(e));
+    return tlfr::query_samples_noalloc(c, d_xyi, n, d_rgba, d_overflow);
+}
+
 tlfr_status tlfr_trace_queries(tlfr_ctx* ctx, const int* xyi, int n, float* rgba, int* trace, int stride)
 {
     if (!ctx || (n > 0 && (!xyi || !rgba || !trace || stride < 2)))

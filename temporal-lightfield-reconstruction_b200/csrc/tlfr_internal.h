@@ -180,6 +180,8 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records);
 // query: all output samples of the frame into rgba (device pointer).
 tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats);
 tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h_trace, int stride);
+// output samples through the full path with working storage in a fixed device array
+tlfr_status query_samples_noalloc(Ctx& c, const int* d_xyi, int n, float* d_rgba, int* d_overflow);
 // host-side output pattern (Reconstruction.cpp:452-512)
 void generate_output_pattern(int out_spp, bool override_uvt, const float* uvt, std::vector<float>& out5);
 

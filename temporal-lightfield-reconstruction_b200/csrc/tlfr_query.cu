@@ -22,6 +22,8 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 namespace tlfr
 {
@@ -1028,6 +1030,132 @@ tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h
     } while (0);
     cudaFree(d_xyi); cudaFree(d_rgba); cudaFree(d_trace); cudaFree(arena);
     return st;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free output-sample queries.
+//
+// Callers that must not allocate device memory while they run (a renderer that
+// reserves all its memory up front, a host thread that must not block on the
+// allocator, code that owns the device heap through its own allocator) can still
+// reconstruct individual output samples.  The per-query working storage that
+// tlfr_trace_queries allocates per call lives here in one fixed device array
+// instead: kNaSlots working slots of kNaSlotBytes each (kNaSlots * kNaSlotBytes
+// = 10.25 MiB), which every device that loads this library keeps until the
+// process exits.  Each slot runs the full per-sample path with capacities
+// kNaStack / kNaLeaf / kNaRs / kNaSurf; a query that needs more is reported as
+// (0, 0, 0, -1) and counted, not retried.
+//
+// All calls share the array: two calls whose kernels overlap on the GPU (on
+// different streams, or from different contexts on the same device) race on it.
+// The kernel needs nothing in the array to start at zero.
+// ---------------------------------------------------------------------------
+namespace
+{
+constexpr int kNaSlots = 256;
+constexpr int kNaStack = 96, kNaLeaf = 512, kNaRs = 2048, kNaSurf = 128;
+constexpr size_t kNaSlotBytes =
+    (sizeof(int) * kNaStack + sizeof(Leaf) * kNaLeaf + sizeof(RSample) * kNaRs + sizeof(Surf) * kNaSurf + 255) &
+    ~(size_t)255;
+constexpr int kNaMaxQueries = 1 << 22;
+constexpr int kNaMaxDevices = 64;
+}
+
+static __device__ __align__(256) unsigned char g_noalloc_arena[kNaSlots * kNaSlotBytes];
+
+namespace
+{
+
+__global__ void __launch_bounds__(64)
+k_query_noalloc(QParams P, const int* __restrict__ xyi, int n, float4* __restrict__ rgba, unsigned char* arena,
+                int* overflow)
+{
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= kNaSlots)
+        return;
+    unsigned char* base = arena + (size_t)slot * kNaSlotBytes;
+    Store S;
+    S.stack = (int*)base;                      S.stack_cap = kNaStack;
+    S.leaves = (Leaf*)(S.stack + kNaStack);    S.leaf_cap = kNaLeaf;
+    S.rs = (RSample*)(S.leaves + kNaLeaf);     S.rs_cap = kNaRs;
+    S.surf = (Surf*)(S.rs + kNaRs);            S.surf_cap = kNaSurf;
+    for (int k = slot; k < n; k += kNaSlots)
+    {
+        const int x = xyi[3 * k], y = xyi[3 * k + 1], i = xyi[3 * k + 2];
+        float4 c = make_float4(0, 0, 0, -1);
+        bool ok = x >= 0 && x < P.W && y >= 0 && y < P.H && i >= 0 && i < P.M;
+        if (ok)
+        {
+            QStats qs{};
+            ok = reconstruct_query<false>(P, S, make_query(P, x, y, i), qs, c, nullptr, 0) == kQOk;
+        }
+        if (!ok)
+        {
+            c = make_float4(0, 0, 0, -1);
+            if (overflow)
+                atomicAdd(overflow, 1);
+        }
+        rgba[k] = c;
+    }
+}
+
+// Device address of g_noalloc_arena for each device, looked up on the first
+// call made with that device current.
+std::mutex g_na_lock;
+void* g_na_ptr[kNaMaxDevices] = {};
+
+} // namespace
+
+tlfr_status query_samples_noalloc(Ctx& c, const int* d_xyi, int n, float* d_rgba, int* d_overflow)
+{
+    if (n < 0 || n > kNaMaxQueries)
+    {
+        c.error = "tlfr_query_samples_noalloc: num_queries " + std::to_string(n) + " outside [0, " +
+                  std::to_string(kNaMaxQueries) + "]";
+        return TLFR_BAD_ARG;
+    }
+    if (c.device < 0 || c.device >= kNaMaxDevices)
+    {
+        c.error = "tlfr_query_samples_noalloc: device ordinal beyond the supported " + std::to_string(kNaMaxDevices);
+        return TLFR_BAD_ARG;
+    }
+    void* arena = nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_na_lock);
+        if (!g_na_ptr[c.device])
+        {
+            // the context's device is current (set by the caller of this function)
+            cudaError_t e = cudaGetSymbolAddress(&g_na_ptr[c.device], g_noalloc_arena);
+            if (e != cudaSuccess)
+            {
+                g_na_ptr[c.device] = nullptr;
+                c.error = std::string("tlfr_query_samples_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+                return TLFR_CUDA;
+            }
+        }
+        arena = g_na_ptr[c.device];
+    }
+    if (d_overflow)
+    {
+        cudaError_t e = cudaMemsetAsync(d_overflow, 0, sizeof(int), c.stream);
+        if (e != cudaSuccess)
+        {
+            c.error = std::string("tlfr_query_samples_noalloc: ") + cudaGetErrorString(e);
+            return TLFR_CUDA;
+        }
+    }
+    if (n == 0)
+        return TLFR_OK;
+    QParams P = make_params(c);
+    TLFR_LAUNCH(c, k_query_noalloc, kNaSlots / 64, 64, c.stream, P, d_xyi, n, reinterpret_cast<float4*>(d_rgba),
+                static_cast<unsigned char*>(arena), d_overflow);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+    {
+        c.error = std::string("tlfr_query_samples_noalloc: ") + cudaGetErrorString(e);
+        return TLFR_CUDA;
+    }
+    return TLFR_OK;
 }
 
 } // namespace tlfr

@@ -104,6 +104,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_tree_export": (ctypes.c_int, [_VP, _FP, _IP, _FP, _IP]),
         "tlfr_output_samples": (ctypes.c_int, [_VP, _FP]),
         "tlfr_trace_queries": (ctypes.c_int, [_VP, _IP, ctypes.c_int, _FP, _IP, ctypes.c_int]),
+        "tlfr_query_samples_noalloc": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
         "tlfr_synth_scene": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_ulonglong, _FP, _FP]),
     }
