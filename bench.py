@@ -274,7 +274,7 @@ def main():
     for _ in range(args.e2e_steps):
         tg.rebuild_from(buf)
         tg.reconstructDofMotion(img)
-    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    e2e_s = (time.perf_counter() - t0) / max(1, args.e2e_steps)
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -355,7 +355,7 @@ void free_ctx_buffers(tlfr::Ctx& c)
                      c.cell_count, c.cell_start, c.cell_items, c.kd, c.kd_level, c.kd_leaves_ordered, c.perm, c.box,
                      c.sbounds, c.surface, c.pending, c.leaf_task_rank, c.ordered_n, c.ordered_prefmax, c.top,
                      c.nodes, c.node_tspan, c.s_pos, c.s_mot, c.s_col, c.s_id, c.d_pattern, c.accum, c.qcol, c.heavy_queue, c.ovf_queue,
-                     c.ovf_scratch, c.d_stats, c.d_out };
+                     c.ovf_scratch, c.coop_scratch, c.d_stats, c.d_out };
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.ev0) cudaEventDestroy(c.ev0);

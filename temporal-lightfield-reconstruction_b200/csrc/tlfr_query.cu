@@ -510,8 +510,8 @@ constexpr int kLStack = 96, kLLeaf = 128;
 // cases, and the first surface is the resolved one).  The first surface's tent
 // filter is accumulated while its samples are accepted, in acceptance order,
 // which is the order the reference filters them in, so no per-sample list is
-// kept.  Returns 0 with the colour in out, or 1 when the output sample needs
-// the full path (2R fetch, or the leaf list outgrew its capacity).
+// kept.  Returns 0 with the colour in out, 1 when the output sample needs the
+// 2R fetch, 2 when the traversal outgrew this pass's capacities.
 TLFR_HD int light_query(const QParams& P, int* stack, Leaf* leaves, const Query& o, float4& out)
 {
     const float R = P.disp0;
@@ -526,7 +526,7 @@ TLFR_HD int light_query(const QParams& P, int* stack, Leaf* leaves, const Query&
             if (node.d.x < 0)
             {
                 if (nleaves == kLLeaf)
-                    return 1;
+                    return 2;
                 const int s0 = node.d.z;
                 const float4 sp0 = P.s_pos[s0];
                 const float mvw = P.s_mot[s0].z;
@@ -537,7 +537,7 @@ TLFR_HD int light_query(const QParams& P, int* stack, Leaf* leaves, const Query&
             else
             {
                 if (sp + 2 > kLStack)
-                    return 1;
+                    return 2;
                 stack[sp++] = node.d.x;
                 stack[sp++] = node.d.y;
             }
@@ -670,7 +670,11 @@ __device__ __forceinline__ void warp_append(int* queue, int* count, bool pred, i
 }
 
 // Pass 1: every output sample through the light path; the rest are queued.
-// Query id q = pixel * M + i.  The queue holds up to num_queries entries.
+// Query id q = pixel * M + i.  The queue holds up to num_queries entries; an
+// entry with kQueueRestart set outgrew the light pass's capacities, so it is
+// not known to need the 2R fetch and the full path starts it over.
+constexpr int kQueueRestart = 1 << 30;
+
 __global__ void __launch_bounds__(kBlock)
 k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
               int* __restrict__ heavy_count)
@@ -681,42 +685,467 @@ k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* 
     {
         const long long q = base + threadIdx.x;
         bool hv = false;
+        int entry = 0;
         if (q < num_queries)
         {
             float4 c;
-            if (light_query(P, stack, leaves, query_of(P, q), c) == 0)
+            const int r = light_query(P, stack, leaves, query_of(P, q), c);
+            if (r == 0)
                 qcol[q] = c;
             else
+            {
                 hv = true;
+                entry = (int)q | (r == 2 ? kQueueRestart : 0);
+            }
         }
-        warp_append(heavy, heavy_count, hv, (int)q);
+        warp_append(heavy, heavy_count, hv, entry);
     }
 }
 
-// Pass 2: the queued output samples through the full path (RO.cpp:50-359).
-// Samples that outgrow these capacities go to the large-capacity pass.
-__global__ void __launch_bounds__(kBlock)
-k_query_heavy(QParams P, const int* __restrict__ heavy, const int* __restrict__ heavy_count,
-              float4* __restrict__ qcol, int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap)
+// ---------------------------------------------------------------------------
+// Pass 2, warp-cooperative: output samples known to need the 2R fetch (the
+// light pass found fetch2R true, RO.cpp:99).  A warp takes 32 queued samples:
+//   1. each lane traverses the hierarchy at 2R for its own sample and sorts its
+//      leaves (32 independent traversals hide each other's latency);
+//   2. then, one sample at a time, the 32 lanes scan that sample's leaves
+//      together: 32 samples tested per step, accepted ones appended in order with
+//      a ballot, surface separation tested against up to 32 earlier leaves per
+//      step (RO.cpp:427-503); the widening fetches when 2R found nothing
+//      (RO.cpp:110-120, lane 0 traverses); tiny-surface merging; per surface
+//      front to back the triangle search spread over the lanes (any covering
+//      triangle settles it, the search order does not change the answer); the
+//      tent filter's products in parallel and their sum in sample order by one
+//      lane (RO.cpp:137-304).
+// Working lists live in a per-warp region of a global arena.  A sample that
+// outgrows them goes to the large-capacity pass, which starts it over.
+// ---------------------------------------------------------------------------
+constexpr int kCWarps = 4;
+constexpr int kCLeaf = 256;         // leaves per lane's traversal
+constexpr int kCRs = 4096;          // accepted samples per sample
+constexpr int kCSurf = 512;         // surfaces per sample
+constexpr int kCStack = 96;
+
+struct CoopScratch
 {
-    int stack[kStackCap];
-    Leaf leaves[kLeafCap];
-    RSample rs[kRsCap];
-    Surf surf[kSurfCap];
-    Store S{ stack, kStackCap, leaves, kLeafCap, rs, kRsCap, surf, kSurfCap };
-    const int n = *heavy_count;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    Leaf    leaves[32][kCLeaf];
+    RSample rs[kCRs];
+    float4  prod[kCRs];
+    Surf    surf[kCSurf];
+};
+
+__device__ __forceinline__ unsigned lanes_below(int lane) { return (1u << lane) - 1u; }
+
+// Reprojection of sample i to the query's (u,v,t) and its squared distance
+// (RO.cpp:436-454); the same operations as collect().
+__device__ __forceinline__ float reproject(const QParams& P, int i, const Query& o, float& x, float& y)
+{
+    const float4 sp4 = P.s_pos[i];
+    const float4 sm = P.s_mot[i];
+    if (sm.x != 0.0f || sm.y != 0.0f || sm.z != 0.0f)
     {
-        const int q = heavy[k];
-        QStats qs{};
-        float4 c;
-        if (reconstruct_query<false>(P, S, query_of(P, q), qs, c, nullptr, 0) == kQOk)
-            qcol[q] = c;
-        else
+        const float dt = o.t - sp4.w;
+        const float Px = sp4.x * sp4.z + sm.x * dt;
+        const float Py = sp4.y * sp4.z + sm.y * dt;
+        const float Pw = (1.0f * sp4.z) + sm.z * dt;
+        const float cr = rcp(Pw);
+        const float coc = P.c0 / Pw + P.c1;
+        x = Px * cr + o.u * coc;
+        y = Py * cr + o.v * coc;
+    }
+    else
+    {
+        x = sp4.x + o.u * sm.w;
+        y = sp4.y + o.v * sm.w;
+    }
+    const float dx = x - o.x, dy = y - o.y;
+    return dx * dx + dy * dy;
+}
+
+// DFS traversal into leaves[] with leaf keys (RO.cpp:368-395) and FW::sort of
+// the leaves (RO.cpp:407).  Returns the leaf count or -1 on overflow.
+__device__ int traverse_sorted(const QParams& P, const Query& o, float R, Leaf* leaves, int cap)
+{
+    int stack[kCStack];
+    int nleaves = 0, sp = 0;
+    stack[sp++] = P.root;
+    while (sp > 0)
+    {
+        const int ni = stack[--sp];
+        const QNode node = P.nodes[ni];
+        if (node_intersect(node, o, R))
         {
-            int slot = atomicAdd(ovf_count, 1);
+            if (node.d.x < 0)
+            {
+                if (nleaves == cap)
+                    return -1;
+                const int s0 = node.d.z;
+                const float4 sp0 = P.s_pos[s0];
+                const float mvw = P.s_mot[s0].z;
+                leaves[nleaves].node = ni;
+                leaves[nleaves].key = sp0.z + (o.t - sp0.w) * mvw;
+                nleaves++;
+            }
+            else
+            {
+                if (sp + 2 > kCStack)
+                    return -1;
+                stack[sp++] = node.d.x;
+                stack[sp++] = node.d.y;
+            }
+        }
+    }
+    LeafSort ls{ leaves };
+    fw_sort(ls, 0, nleaves);
+    return nleaves;
+}
+
+// Cooperative collectInputSamples2 scan (RO.cpp:412-503) over sorted leaves.
+// All lanes call it with the same arguments; returns the accepted count (same
+// on all lanes) or -1 when rs / surf outgrow the scratch.
+__device__ int coop_scan(const QParams& P, const Query& o, float R, const Leaf* leaves, int nleaves,
+                         CoopScratch& S, int& nsurf_out)
+{
+    const int lane = threadIdx.x & 31;
+    const float RANGE = 1.0f / sqrtf(128.0f);
+    const float uvtmin[3] = { o.u - RANGE, o.v - RANGE, o.t - 0.5f * RANGE };
+    const float uvtmax[3] = { o.u + RANGE, o.v + RANGE, o.t + 0.5f * RANGE };
+    const float R2 = R * R;
+    int nsurf = 0, nrs = 0, surfaceStart = 0;
+    // the open surface's running state, identical on all lanes
+    float minDist = kF32Max;
+    int minIndex = -1, quad = 0, sstart = 0;
+    for (int lidx = 0; lidx < nleaves; lidx++)
+    {
+        const QNode node = P.nodes[leaves[lidx].node];
+        const int s0 = node.d.z, s1 = node.d.w;
+        bool first = true;
+        for (int base = s0; base < s1; base += 32)
+        {
+            const int i = base + lane;
+            float x = 0, y = 0, d2 = 0;
+            bool acc = false;
+            if (i < s1)
+            {
+                d2 = reproject(P, i, o, x, y);
+                acc = d2 <= R2;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, acc);
+            if (!m)
+                continue;
+            if (first)
+            {
+                first = false;
+                bool same = true;
+                for (int jb = surfaceStart; jb < lidx && same; jb += 32)
+                {
+                    const int j = jb + lane;
+                    const bool ok = (j < lidx) ? same_surface(node, P.nodes[leaves[j].node], uvtmin, uvtmax) : true;
+                    same = __all_sync(0xffffffffu, ok);
+                }
+                if (!same || nsurf == 0)
+                {
+                    if (nsurf > 0 && lane == 0)
+                    {
+                        Surf& p = S.surf[nsurf - 1];
+                        p.n = nrs - sstart; p.minDist = minDist; p.minIndex = minIndex; p.quad = quad;
+                    }
+                    if (nsurf == kCSurf)
+                        return -1;
+                    surfaceStart = lidx;
+                    nsurf++;
+                    sstart = nrs;
+                    minDist = kF32Max; minIndex = -1; quad = 0;
+                    if (lane == 0) S.surf[nsurf - 1].start = nrs;
+                }
+            }
+            const int cnt = __popc(m);
+            if (nrs + cnt > kCRs)
+                return -1;
+            const int pos = nrs + __popc(m & lanes_below(lane));
+            const float dx = x - o.x, dy = y - o.y;
+            const int rpos = (dx >= 0 ? 1 : 4) | (dy >= 0 ? 2 : 8);
+            if (acc)
+            {
+                RSample r;
+                r.x = x; r.y = y; r.index = i; r.rpos = rpos;
+                S.rs[pos] = r;
+            }
+            quad |= __reduce_or_sync(0xffffffffu, acc ? (1 << (rpos & 3)) : 0);
+            // first strict minimum in acceptance order (RO.cpp:494-499)
+            const float dist = acc ? sqrtf(d2) : kF32Max;
+            float cmin = dist;
+            for (int off = 16; off > 0; off >>= 1)
+                cmin = minr(cmin, __shfl_xor_sync(0xffffffffu, cmin, off));
+            if (cmin < minDist)
+            {
+                const unsigned at = __ballot_sync(0xffffffffu, acc && dist == cmin);
+                const int fl = __ffs(at) - 1;
+                minDist = cmin;
+                minIndex = nrs + __popc(m & lanes_below(fl)) - sstart;
+            }
+            nrs += cnt;
+        }
+    }
+    if (nsurf > 0 && lane == 0)
+    {
+        Surf& p = S.surf[nsurf - 1];
+        p.n = nrs - sstart; p.minDist = minDist; p.minIndex = minIndex; p.quad = quad;
+    }
+    __syncwarp();
+    nsurf_out = nsurf;
+    return nrs;
+}
+
+__device__ __forceinline__ void coop_reverse(RSample* a, int lo, int hi)     // [lo, hi)
+{
+    const int lane = threadIdx.x & 31;
+    const int n = hi - lo;
+    for (int k = lane; k < n / 2; k += 32)
+    {
+        RSample t = a[lo + k];
+        a[lo + k] = a[hi - 1 - k];
+        a[hi - 1 - k] = t;
+    }
+    __syncwarp();
+}
+
+// Moves (m, k) forward by step pairs in the m-major order of pairs
+// m < k <= n-2; m > n-3 afterwards means past the last pair.
+__device__ __forceinline__ void pair_advance(int n, int step, int& m, int& k)
+{
+    k += step;
+    while (m <= n - 3 && k > n - 2)
+    {
+        const int over = k - (n - 1);
+        m++;
+        k = m + 1 + over;
+    }
+}
+
+// Any triangle of rs[0..n) covering o (RO.cpp:221-259), searched by all lanes:
+// lane l takes pairs l, l+32, ... and the third vertices after each.
+__device__ bool coop_triangle(const RSample* in, int n, const Query& o, float dispersion)
+{
+    const int lane = threadIdx.x & 31;
+    const int pairs = (n - 2) * (n - 1) / 2;
+    bool found = false;
+    int m = 0, k = 1;
+    pair_advance(n, lane, m, k);
+    for (int pb = 0; pb < pairs; pb += 32, pair_advance(n, 32, m, k))
+    {
+        if (m <= n - 3)
+        {
+            const RSample r0 = in[m], r1 = in[k];
+            const int rp01 = r0.rpos | r1.rpos;
+            if (!(len2(r0.x - r1.x, r0.y - r1.y) > 2 * dispersion))
+            {
+                for (int l = k + 1; l < n && !found; l++)
+                {
+                    const RSample r2 = in[l];
+                    if ((rp01 | r2.rpos) != 15)
+                        continue;
+                    if (len2(r0.x - r2.x, r0.y - r2.y) > 2 * dispersion ||
+                        len2(r1.x - r2.x, r1.y - r2.y) > 2 * dispersion)
+                        continue;
+                    if (len2(r0.x - o.x, r0.y - o.y) > dispersion && len2(r1.x - o.x, r1.y - o.y) > dispersion &&
+                        len2(r2.x - o.x, r2.y - o.y) > dispersion)
+                        continue;
+                    EdgeFn e0 = edge_make(r1.x, r1.y, r2.x, r2.y);
+                    EdgeFn e1 = edge_make(r2.x, r2.y, r0.x, r0.y);
+                    EdgeFn e2 = edge_make(r0.x, r0.y, r1.x, r1.y);
+                    bool p0 = edge_test(e0, o.x, o.y);
+                    bool p1 = edge_test(e1, o.x, o.y);
+                    bool p2 = edge_test(e2, o.x, o.y);
+                    found = (p0 && p1 && p2) || (!p0 && !p1 && !p2);
+                }
+            }
+        }
+        if (__any_sync(0xffffffffu, found))
+            return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(kCWarps * 32)
+k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ queue_count,
+             float4* __restrict__ qcol, int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap,
+             CoopScratch* __restrict__ scratch)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.x * kCWarps + (threadIdx.x >> 5);
+    const int nwarps = gridDim.x * kCWarps;
+    CoopScratch& S = scratch[warp];
+    const int n = *queue_count;
+    for (int b = warp * 32; b < n; b += nwarps * 32)
+    {
+        // 1. per-lane 2R traversal and leaf sort; entries that outgrew the light
+        // pass go to the large-capacity pass
+        const int entry = (b + lane < n) ? queue[b + lane] : -1;
+        const bool restart = entry >= 0 && (entry & kQueueRestart);
+        if (restart)
+        {
+            const int slot = atomicAdd(ovf_count, 1);
             if (slot < ovf_cap)
-                ovf_queue[slot] = q;
+                ovf_queue[slot] = entry & ~kQueueRestart;
+        }
+        const bool valid = entry >= 0 && !restart;
+        const int myq = valid ? entry : 0;
+        Query myo = query_of(P, myq);
+        int mycount = valid ? traverse_sorted(P, myo, P.disp0 * 2, S.leaves[lane], kCLeaf) : 0;
+        __syncwarp();
+        // 2. each sample of the batch by the whole warp
+        for (int j = 0; j < 32; j++)
+        {
+            const bool vj = __shfl_sync(0xffffffffu, valid, j);
+            if (!vj)
+                continue;
+            const int qj = __shfl_sync(0xffffffffu, myq, j);
+            int nl = __shfl_sync(0xffffffffu, mycount, j);
+            bool ovf = nl < 0;
+            Query o;
+            o.x = __shfl_sync(0xffffffffu, myo.x, j);
+            o.y = __shfl_sync(0xffffffffu, myo.y, j);
+            o.u = __shfl_sync(0xffffffffu, myo.u, j);
+            o.v = __shfl_sync(0xffffffffu, myo.v, j);
+            o.t = __shfl_sync(0xffffffffu, myo.t, j);
+            float dispersion = P.disp0;
+            int nsurf = 0, total = 0;
+            if (!ovf)
+            {
+                total = coop_scan(P, o, dispersion * 2, S.leaves[j], nl, S, nsurf);
+                ovf = total < 0;
+            }
+            // widening when 2R found nothing (RO.cpp:110-120); lane 0 traverses
+            for (int k = 0; k < 3 && !ovf && total == 0; k++)
+            {
+                dispersion *= 2.f;
+                int cnt = 0;
+                if (lane == 0)
+                    cnt = traverse_sorted(P, o, dispersion * 2, S.leaves[j], kCLeaf);
+                cnt = __shfl_sync(0xffffffffu, cnt, 0);
+                __syncwarp();
+                if (cnt < 0) { ovf = true; break; }
+                total = coop_scan(P, o, dispersion * 2, S.leaves[j], cnt, S, nsurf);
+                ovf = total < 0;
+            }
+            if (ovf)
+            {
+                if (lane == 0)
+                {
+                    int slot = atomicAdd(ovf_count, 1);
+                    if (slot < ovf_cap)
+                        ovf_queue[slot] = qj;
+                }
+                __syncwarp();
+                continue;
+            }
+            // tiny-surface merging (RO.cpp:137-156): dst.samples += src.samples
+            for (int sidx = 0; sidx < nsurf - 1; sidx++)
+            {
+                Surf src = S.surf[sidx], dst = S.surf[sidx + 1];
+                __syncwarp();
+                if (src.n < 4)
+                {
+                    const int lo = src.start, mid = src.start + src.n, hi = dst.start + dst.n;
+                    if (src.n > 0 && mid == dst.start)
+                    {
+                        coop_reverse(S.rs, lo, mid);
+                        coop_reverse(S.rs, mid, hi);
+                        coop_reverse(S.rs, lo, hi);
+                    }
+                    if (lane == 0)
+                    {
+                        Surf& d = S.surf[sidx + 1];
+                        d.start = lo;
+                        d.n = hi - lo;
+                        if (src.minDist < dst.minDist)
+                        {
+                            d.minDist = src.minDist;
+                            d.minIndex = src.minIndex;
+                        }
+                        S.surf[sidx].n = 0;
+                    }
+                    __syncwarp();
+                }
+            }
+            // resolve (RO.cpp:165-304)
+            bool found = false;
+            float4 res = make_float4(0, 0, 0, 0);
+            float nearestDist = kF32Max;
+            int nearS = -1, nearI = 1;
+            for (int sidx = 0; sidx < nsurf && !found; sidx++)
+            {
+                const Surf sf = S.surf[sidx];
+                const int cnt = sf.n;
+                if (cnt == 0)
+                    continue;
+                const RSample* in = S.rs + sf.start;
+                if (sf.minDist < nearestDist)
+                {
+                    nearestDist = sf.minDist;
+                    nearS = sidx; nearI = sf.minIndex;
+                }
+                if (sf.minDist < 0.f || sidx == nsurf - 1)
+                    found = true;
+                if (cnt >= 200)
+                    found = true;
+                if (!found)
+                    found = coop_triangle(in, cnt, o, dispersion);
+                if (found)
+                {
+                    for (int k = lane; k < cnt; k += 32)
+                    {
+                        const RSample r = in[k];
+                        const float dx = o.x - r.x, dy = o.y - r.y;
+                        const float weight = 1 - len2(dx, dy) / dispersion;
+                        // alpha is 1 (forced at load), so an included sample has pr.w = weight > 0;
+                        // pr.w = -1 marks a sample the reference skips (weight <= 0)
+                        float4 pr = make_float4(0, 0, 0, -1.0f);
+                        if (weight > 0)
+                        {
+                            const float4 c = P.s_col[r.index];
+                            pr = make_float4(c.x * weight, c.y * weight, c.z * weight, c.w * weight);
+                        }
+                        S.prod[k] = pr;
+                    }
+                    __syncwarp();
+                    if (lane == 0)
+                    {
+                        for (int k = 0; k < cnt; k++)
+                        {
+                            const float4 pr = S.prod[k];
+                            if (pr.w < 0)
+                                continue;
+                            res.x += pr.x; res.y += pr.y; res.z += pr.z; res.w += pr.w;
+                        }
+                        const float oow = rcp(res.w);
+                        res.x *= oow; res.y *= oow; res.z *= oow; res.w *= oow;
+                    }
+                    nearS = sidx; nearI = sf.minIndex;
+                }
+            }
+            if (lane == 0)
+            {
+                float4 out = make_float4(0, 0, 0, 0);
+                if (nearS != -1)
+                {
+                    if (res.w == 0)
+                        res = P.s_col[S.rs[S.surf[nearS].start + nearI].index];
+                    if (P.lens_filter == 1)
+                    {
+                        float g = gaussian(o.u, 0.5f, 0) * gaussian(o.v, 0.5f, 0);
+                        res.x *= g; res.y *= g; res.z *= g; res.w *= g;
+                    }
+                    if (P.time_filter == 1)
+                    {
+                        float g = gaussian(o.t, 0.25f, 0.5f);
+                        res.x *= g; res.y *= g; res.z *= g; res.w *= g;
+                    }
+                    out = res;
+                }
+                qcol[qj] = out;
+            }
+            __syncwarp();
         }
     }
 }
@@ -876,9 +1305,9 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
     cudaStream_t s = c.stream;
     const long long npix = (long long)c.W * c.H;
     const long long nq = npix * c.out_spp;
-    if (nq >= (1ll << 31))
+    if (nq >= kQueueRestart)
     {
-        c.error = "more than 2^31 output samples in one frame";
+        c.error = "more than 2^30 output samples in one frame";
         return TLFR_BAD_ARG;
     }
     if ((size_t)nq > c.qcol_cap)
@@ -914,10 +1343,16 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
     }
     else
     {
+        const int coop_blocks = 148 * 4;
+        if (!c.coop_scratch)
+        {
+            c.coop_scratch_bytes = sizeof(CoopScratch) * coop_blocks * kCWarps;
+            CKQ(cudaMalloc(&c.coop_scratch, c.coop_scratch_bytes));
+        }
         TLFR_LAUNCH(c, k_query_light, blocks, kBlock, s, P, nq, c.qcol, c.heavy_queue, counters + 2);
         CKQ(cudaEventRecord(c.evq1, s));
-        TLFR_LAUNCH(c, k_query_heavy, 148 * 16, kBlock, s, P, c.heavy_queue, counters + 2, c.qcol, c.ovf_queue,
-                    counters + 0, (int)c.ovf_cap);
+        TLFR_LAUNCH(c, k_query_coop, coop_blocks, kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol,
+                    c.ovf_queue, counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(c.coop_scratch));
     }
     CKQ(cudaEventRecord(c.evq2, s));
     CKQ(cudaGetLastError());
