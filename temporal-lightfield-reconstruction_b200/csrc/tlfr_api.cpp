@@ -354,7 +354,7 @@ void free_ctx_buffers(tlfr::Ctx& c)
     void* ptrs[] = { c.own_records ? c.d_records : nullptr, c.rp_pos, c.rp_mot, c.rp_cell, c.hits, c.d_grid,
                      c.cell_count, c.cell_start, c.cell_items, c.kd, c.kd_level, c.kd_leaves_ordered, c.perm, c.box,
                      c.sbounds, c.surface, c.pending, c.leaf_task_rank, c.ordered_n, c.ordered_prefmax, c.top,
-                     c.nodes, c.node_tspan, c.s_pos, c.s_mot, c.s_col, c.s_id, c.d_pattern, c.accum, c.qcol, c.heavy_queue, c.ovf_queue,
+                     c.nodes, c.node_tspan, c.s_rec, c.s_col, c.s_id, c.d_pattern, c.accum, c.qcol, c.heavy_queue, c.ovf_queue,
                      c.ovf_scratch, c.coop_scratch, c.d_stats, c.d_out };
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -828,13 +828,12 @@ tlfr_status tlfr_tree_export(tlfr_ctx* ctx, float* nodef, int* nodei, float* sam
     const int nn = c.num_nodes, ns = c.num_samples;
     std::vector<tlfr::QNode> q(nn);
     std::vector<float2> ts(nn);
-    std::vector<float4> p(ns), m(ns), col(ns);
+    std::vector<float4> rec2(2 * (size_t)ns), col(ns);
     std::vector<int> id(ns);
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMemcpy(q.data(), c.nodes, sizeof(tlfr::QNode) * nn, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(ts.data(), c.node_tspan, sizeof(float2) * nn, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(p.data(), c.s_pos, sizeof(float4) * ns, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(m.data(), c.s_mot, sizeof(float4) * ns, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(rec2.data(), c.s_rec, sizeof(float4) * 2 * ns, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(col.data(), c.s_col, sizeof(float4) * ns, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(id.data(), c.s_id, sizeof(int) * ns, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess)
@@ -885,10 +884,12 @@ tlfr_status tlfr_tree_export(tlfr_ctx* ctx, float* nodef, int* nodei, float* sam
         if (samplef)
         {
             float* f = samplef + (size_t)j * 12;
-            f[0] = p[j].x; f[1] = p[j].y; f[2] = p[j].z; f[3] = p[j].w;
-            f[4] = m[j].x; f[5] = m[j].y; f[6] = m[j].z;
+            const float4& p = rec2[2 * (size_t)j];
+            const float4& m = rec2[2 * (size_t)j + 1];
+            f[0] = p.x; f[1] = p.y; f[2] = p.z; f[3] = p.w;
+            f[4] = m.x; f[5] = m.y; f[6] = m.z;
             f[7] = col[j].x; f[8] = col[j].y; f[9] = col[j].z; f[10] = col[j].w;
-            f[11] = p[j].z;     // key = w after reprojection (Reconstruction.hpp:119)
+            f[11] = p.z;     // key = w after reprojection (Reconstruction.hpp:119)
         }
         if (sample_ids) sample_ids[j] = id[j];
     }

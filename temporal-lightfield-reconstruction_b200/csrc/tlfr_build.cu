@@ -513,7 +513,7 @@ __global__ void k_leaf_prepare(const int* __restrict__ leaves_ordered, int num_l
                                const float4* __restrict__ rp_pos, const float4* __restrict__ rp_mot,
                                const float4* __restrict__ rec, float W, float H, float c0, float c1,
                                int* __restrict__ perm, float* __restrict__ box, Bounds* __restrict__ sbounds,
-                               float4* __restrict__ s_pos, float4* __restrict__ s_mot, float4* __restrict__ s_col,
+                               float4* __restrict__ s_rec, float4* __restrict__ s_col,
                                int* __restrict__ s_id, int* __restrict__ ordered_n, int* invalid_count)
 {
     const int gw = g->gw;
@@ -578,8 +578,8 @@ __global__ void k_leaf_prepare(const int* __restrict__ leaves_ordered, int num_l
             // tree-ordered sample record (Reconstruction.hpp:73-86 Sample, color alpha 1)
             float4 r1 = __ldg(&rec[(size_t)id * 4 + 1]);
             float4 r2 = __ldg(&rec[(size_t)id * 4 + 2]);
-            s_pos[off + j] = p;
-            s_mot[off + j] = make_float4(mv[0], mv[1], mv[2], c0 / sw + c1);
+            s_rec[2 * (off + j)] = p;
+            s_rec[2 * (off + j) + 1] = make_float4(mv[0], mv[1], mv[2], c0 / sw + c1);
             s_col[off + j] = make_float4(r1.w, r2.x, r2.y, 1.0f);
             s_id[off + j] = id;
         }
@@ -710,7 +710,7 @@ __device__ __forceinline__ void bounds_from_bnode(Bounds& b, const BNode& n)
 
 // Leaf construction, part 2: surface scan and leaf nodes (RTB.cpp:222-378).
 __global__ void k_leaf_scan(const int* __restrict__ leaves_ordered, int num_leaves, KdNode* __restrict__ kd,
-                            const float4* __restrict__ s_pos, const float* __restrict__ box,
+                            const float4* __restrict__ s_rec, const float* __restrict__ box,
                             const Bounds* __restrict__ sbounds, int* __restrict__ surface, BNode* __restrict__ pending)
 {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < num_leaves; r += gridDim.x * blockDim.x)
@@ -742,11 +742,11 @@ __global__ void k_leaf_scan(const int* __restrict__ leaves_ordered, int num_leav
                 for (int q = 0; q < 2; q++)
                     mvmin[q] = 0.5f * (bb[4 + q] + bb[6 + q]) - 0.5f * (bb[q] + bb[2 + q]);
                 mvmax[0] = mvmin[0]; mvmax[1] = mvmin[1];
-                surfacet = s_pos[off + surfacebegin].w;
+                surfacet = s_rec[2 * (off + surfacebegin)].w;
                 reset = false;
             }
             bool conflict = false, early = false;
-            if (surfacet != s_pos[off + cur].w)
+            if (surfacet != s_rec[2 * (off + cur)].w)
             {
                 surfacebegin = cur;
                 surf[cur] = ++currsurface;
@@ -1114,7 +1114,7 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
     if (nacc > c.samp_cap)
     {
         cudaFree(c.perm); cudaFree(c.box); cudaFree(c.sbounds); cudaFree(c.surface); cudaFree(c.pending);
-        cudaFree(c.s_pos); cudaFree(c.s_mot); cudaFree(c.s_col); cudaFree(c.s_id);
+        cudaFree(c.s_rec); cudaFree(c.s_col); cudaFree(c.s_id);
         cudaFree(c.top);
         cudaFree(c.nodes); cudaFree(c.node_tspan);
         c.samp_cap = 0;
@@ -1123,8 +1123,7 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
         CK(cudaMalloc(&c.sbounds, sizeof(Bounds) * nacc));
         CK(cudaMalloc(&c.surface, sizeof(int) * nacc));
         CK(cudaMalloc(&c.pending, sizeof(BNode) * nacc));
-        CK(cudaMalloc(&c.s_pos, sizeof(float4) * nacc));
-        CK(cudaMalloc(&c.s_mot, sizeof(float4) * nacc));
+        CK(cudaMalloc(&c.s_rec, sizeof(float4) * 2 * nacc));
         CK(cudaMalloc(&c.s_col, sizeof(float4) * nacc));
         CK(cudaMalloc(&c.s_id, sizeof(int) * nacc));
         CK(cudaMalloc(&c.top, sizeof(BNode) * kTopCap));
@@ -1146,13 +1145,13 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
     // --- leaves ---
     TLFR_LAUNCH(c, k_leaf_prepare, grid_for(num_leaves, 128), 128, s, 
         c.kd_leaves_ordered, num_leaves, c.kd, c.cell_start, c.cell_items, c.d_grid, c.rp_pos, c.rp_mot, rec,
-        (float)c.W, (float)c.H, c.coc[0], c.coc[1], c.perm, c.box, c.sbounds, c.s_pos, c.s_mot, c.s_col, c.s_id,
+        (float)c.W, (float)c.H, c.coc[0], c.coc[1], c.perm, c.box, c.sbounds, c.s_rec, c.s_col, c.s_id,
         c.ordered_n, counters + 2);
     TLFR_LAUNCH(c, k_task_prefix, 32, 1024, s, c.d_grid, c.ordered_n, c.ordered_prefmax, c.leaf_task_rank);
     TLFR_LAUNCH(c, k_stale_boxes, grid_for(num_leaves, 128), 128, s, c.kd_leaves_ordered, c.d_grid, c.kd, c.ordered_n,
                                                             c.ordered_prefmax, c.leaf_task_rank, c.sbounds, c.box,
                                                             num_leaves, 0);
-    TLFR_LAUNCH(c, k_leaf_scan, grid_for(num_leaves, 128), 128, s, c.kd_leaves_ordered, num_leaves, c.kd, c.s_pos, c.box,
+    TLFR_LAUNCH(c, k_leaf_scan, grid_for(num_leaves, 128), 128, s, c.kd_leaves_ordered, num_leaves, c.kd, c.s_rec, c.box,
                                                           c.sbounds, c.surface, c.pending);
     CK(cudaGetLastError());
 

@@ -143,8 +143,9 @@ struct Ctx
     QNode*  nodes = nullptr;
     float2* node_tspan = nullptr;   // time span per node (tree export only)
     size_t  node_cap = 0;
-    float4* s_pos = nullptr;        // x, y, w, t  (tree order)
-    float4* s_mot = nullptr;        // mv (3), coc radius at w
+    // samples in tree order, one 32-byte record each (a single 256-bit load):
+    // s_rec[2i] = (x, y, w, t), s_rec[2i+1] = (mv (3), coc radius at w)
+    float4* s_rec = nullptr;
     float4* s_col = nullptr;        // rgba
     int*    s_id = nullptr;         // input record index
     int     num_samples = 0;

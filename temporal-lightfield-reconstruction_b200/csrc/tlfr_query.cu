@@ -46,8 +46,7 @@ struct Store
 struct QParams
 {
     const QNode*  nodes;
-    const float4* s_pos;
-    const float4* s_mot;
+    const float4* s_rec;        // 2 per sample: (x, y, w, t), (mv, coc radius at w)
     const float4* s_col;
     const float*  pattern;      // 64 * M * 5
     int   M, W, H, root;
@@ -63,6 +62,21 @@ struct QStats
 };
 
 struct Query { float x, y, u, v, t; };
+
+// Sample record i (32 bytes, 32-byte aligned) in one 256-bit load.
+TLFR_HD void load_sample(const float4* rec, int i, float4& pos, float4& mot)
+{
+#ifdef __CUDA_ARCH__
+    asm("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(pos.x), "=f"(pos.y), "=f"(pos.z), "=f"(pos.w), "=f"(mot.x), "=f"(mot.y), "=f"(mot.z), "=f"(mot.w)
+        : "l"(rec + 2 * (size_t)i));
+#else
+    pos = rec[2 * (size_t)i];
+    mot = rec[2 * (size_t)i + 1];
+#endif
+}
+
+
 
 enum { kQOk = 0, kQOverflow = 1 };
 
@@ -139,8 +153,8 @@ TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& ns
                 if (nleaves == S.leaf_cap)
                     return -1;   // leaf list full
                 const int s0 = node.d.z;
-                const float4 sp0 = P.s_pos[s0];
-                const float mvw = P.s_mot[s0].z;
+                const float4 sp0 = P.s_rec[2 * (s0)];
+                const float mvw = P.s_rec[2 * (s0) + 1].z;
                 S.leaves[nleaves].node = ni;
                 S.leaves[nleaves].key = sp0.z + (o.t - sp0.w) * mvw;
                 nleaves++;
@@ -172,8 +186,8 @@ TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& ns
         st.in_leaves += (unsigned)(s1 - s0);
         for (int i = s0; i < s1; i++)
         {
-            const float4 sp4 = P.s_pos[i];     // x, y, w, t
-            const float4 sm = P.s_mot[i];      // mv, coc(w)
+            float4 sp4, sm;     // (x, y, w, t), (mv, coc(w))
+            load_sample(P.s_rec, i, sp4, sm);
             float x, y, w;
             if (sm.x != 0.0f || sm.y != 0.0f || sm.z != 0.0f)
             {
@@ -500,75 +514,210 @@ __device__ void flush_stats(const QStats& st, DevStats* ds)
 constexpr int kBlock = 128;
 // capacities of the full per-query path (statistics pass and heavy pass)
 constexpr int kStackCap = 96, kLeafCap = 256, kRsCap = 512, kSurfCap = 64;
-// capacities of the light pass
-constexpr int kLStack = 96, kLLeaf = 128;
+// capacities of the light pass: traversal stack and leaf list per output
+// sample, both in shared memory
+constexpr int kLStack = 16, kLLeaf = 32;
 
-// Light pass (RO.cpp:94-99, 165-304 for the common case): the 1R fetch when it
-// settles the output sample by itself, i.e. when it ends with exactly one
-// surface, or when the first surface already holds samples in all four
-// quadrants by the time a second surface opens (fetch2R is false in both
-// cases, and the first surface is the resolved one).  The first surface's tent
-// filter is accumulated while its samples are accepted, in acceptance order,
-// which is the order the reference filters them in, so no per-sample list is
-// kept.  Returns 0 with the colour in out, 1 when the output sample needs the
-// 2R fetch, 2 when the traversal outgrew this pass's capacities.
-TLFR_HD int light_query(const QParams& P, int* stack, Leaf* leaves, const Query& o, float4& out)
+// Per-thread column of a shared-memory array laid out [slot][thread]: a warp
+// whose lanes touch different slots still hits distinct banks.  The host build
+// (stride 1) runs the same code on a plain array.
+template <class T>
+struct Column
+{
+    T* base;
+    int stride;
+    TLFR_HD T& operator[](int k) const { return base[k * stride]; }
+};
+
+TLFR_HD float int_as_float_bits(int v)
+{
+#ifdef __CUDA_ARCH__
+    return __int_as_float(v);
+#else
+    float f;
+    memcpy(&f, &v, 4);
+    return f;
+#endif
+}
+TLFR_HD int float_as_int_bits(float v)
+{
+#ifdef __CUDA_ARCH__
+    return __float_as_int(v);
+#else
+    int i;
+    memcpy(&i, &v, 4);
+    return i;
+#endif
+}
+
+// A leaf found by the light pass's traversal: (sort key = w at the output
+// sample's time (RO.cpp:390-392), node index as bits).
+struct LLeafSort
+{
+    Column<float2> l;
+    TLFR_HD int cmp(int a, int b) const { const float ka = l[a].x, kb = l[b].x; return (ka < kb) ? -1 : (ka > kb) ? 1 : 0; }
+    TLFR_HD void swap(int a, int b) { const float2 t = l[a]; l[a] = l[b]; l[b] = t; }
+};
+TLFR_HD int leaf_node(const Column<float2>& leaves, int k) { return float_as_int_bits(leaves[k].y); }
+
+// Appends leaf node ni (first sample s0) with its key; false when full.
+TLFR_HD bool light_append(const QParams& P, const Query& o, const Column<float2>& leaves, int& nleaves, int ni, int s0)
+{
+    if (nleaves == kLLeaf)
+        return false;
+    const float4 sp0 = P.s_rec[2 * (s0)];
+    const float mvw = P.s_rec[2 * (s0) + 1].z;
+    leaves[nleaves++] = make_float2(sp0.z + (o.t - sp0.w) * mvw, int_as_float_bits(ni));
+    return true;
+}
+
+// Light pass, part 1 (RO.cpp:368-407), one output sample per thread: DFS in
+// the reference's order (push child0, child1, pop the last) into the leaf
+// column, then FW::sort of the leaves by key.  Children are stored as pairs,
+// so a node that intersects has both children loaded and tested together and
+// only those that intersect are pushed (a leaf child waits on the stack only
+// behind an internal child1).  The loop has no early exit (an overflow sets a
+// flag), so a warp reconverges at the end of every step.  Returns the leaf
+// count, or -1 when the stack or the leaf column is full.
+TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Column<float2>& leaves, const Query& o)
 {
     const float R = P.disp0;
     int nleaves = 0, sp = 0;
-    stack[sp++] = P.root;
-    while (sp > 0)
+    bool ok = true;
     {
-        const int ni = stack[--sp];
-        const QNode node = P.nodes[ni];
-        if (node_intersect(node, o, R))
+        const QNode rn = P.nodes[P.root];
+        if (node_intersect(rn, o, R))
         {
-            if (node.d.x < 0)
+            if (rn.d.x < 0)
+                ok = light_append(P, o, leaves, nleaves, P.root, rn.d.z);
+            else
+                stack[sp++] = rn.d.x;
+        }
+    }
+    // stack entries: >= 0 the first child of an intersecting internal node;
+    // < 0 (~node) an intersecting leaf
+    while (sp > 0 && ok)
+    {
+        const int e = stack[--sp];
+        if (e < 0)
+            ok = light_append(P, o, leaves, nleaves, ~e, P.nodes[~e].d.z);
+        else
+        {
+            const QNode n0 = P.nodes[e];
+            const QNode n1 = P.nodes[e + 1];
+            const bool h0 = node_intersect(n0, o, R);
+            const bool h1 = node_intersect(n1, o, R);
+            if (h1 && n1.d.x >= 0)
             {
-                if (nleaves == kLLeaf)
-                    return 2;
-                const int s0 = node.d.z;
-                const float4 sp0 = P.s_pos[s0];
-                const float mvw = P.s_mot[s0].z;
-                leaves[nleaves].node = ni;
-                leaves[nleaves].key = sp0.z + (o.t - sp0.w) * mvw;
-                nleaves++;
+                // child1's subtree comes first; child0 waits below it
+                if (sp + 2 > kLStack)
+                    ok = false;
+                else
+                {
+                    if (h0)
+                        stack[sp++] = n0.d.x >= 0 ? n0.d.x : ~e;
+                    stack[sp++] = n1.d.x;
+                }
             }
             else
             {
-                if (sp + 2 > kLStack)
-                    return 2;
-                stack[sp++] = node.d.x;
-                stack[sp++] = node.d.y;
+                if (h1)
+                    ok = light_append(P, o, leaves, nleaves, e + 1, n1.d.z);
+                if (h0 && ok)
+                {
+                    if (n0.d.x < 0)
+                        ok = light_append(P, o, leaves, nleaves, e, n0.d.z);
+                    else if (sp + 1 > kLStack)
+                        ok = false;
+                    else
+                        stack[sp++] = n0.d.x;
+                }
             }
         }
     }
-    LeafSort ls{ leaves };
+    if (!ok)
+        return -1;
+    LLeafSort ls{ leaves };
     fw_sort(ls, 0, nleaves);
+    return nleaves;
+}
 
+// Light pass, part 2 (RO.cpp:94-99, 165-304 for the common case): the 1R scan
+// of one output sample's sorted leaves by the whole warp, lanes over
+// consecutive samples of a leaf (coalesced 32-byte records).  It settles the
+// output sample when the 1R fetch ends with exactly one surface, or when the
+// first surface holds samples in all four quadrants by the time a second one
+// opens (fetch2R is false in both cases and the first surface is resolved).
+// Accepted samples update the surface state in sample order: quadrant mask,
+// first strict minimum distance, and the tent filter, summed in acceptance
+// order (the reference's filter order, RO.cpp:274-294).  At the first accepted
+// sample of a later leaf, sameSurface (Reconstruction.hpp:457-525) is tested
+// against every leaf since the surface opened (RO.cpp:465-470), lanes over
+// those leaves; when one fails the scan stops there.  All lanes call it with
+// the same arguments and get the same result: 0 with the colour in out, 1
+// when the output sample needs the 2R fetch.
+__device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, int nleaves, const Query& o,
+                               float4& out)
+{
+    const int lane = threadIdx.x & 31;
+    const float R = P.disp0;
+    const float R2 = R * R;
     const float RANGE = 1.0f / sqrtf(128.0f);
     const float uvtmin[3] = { o.u - RANGE, o.v - RANGE, o.t - 0.5f * RANGE };
     const float uvtmax[3] = { o.u + RANGE, o.v + RANGE, o.t + 0.5f * RANGE };
-    const float R2 = R * R;
-    int nsurf = 0, surfaceStart = 0, quad = 0, nearest = -1;
+    // sample range of leaf k, held by lane k (the leaf column holds at most 32)
+    int my_s0 = 0, my_s1 = 0;
+    if (lane < nleaves)
+    {
+        const int4 d = P.nodes[leaf_node(leaves, lane)].d;
+        my_s0 = d.z;
+        my_s1 = d.w;
+    }
+    const unsigned nonempty = __ballot_sync(0xffffffffu, my_s0 != my_s1);
+    // chunks of 32 consecutive samples of one leaf, in leaf order; the next
+    // chunk's records are loaded while the current one is processed
+    auto next_leaf = [&](int k) { const unsigned m = nonempty & ~((2u << k) - 1u); return m ? __ffs(m) - 1 : 32; };
+    int lidx = (nonempty & 1u) ? 0 : next_leaf(0);
+    int b = __shfl_sync(0xffffffffu, my_s0, lidx & 31);
+    int s1 = __shfl_sync(0xffffffffu, my_s1, lidx & 31);
+    float4 cpos = make_float4(0, 0, 0, 0), cmot = cpos, ccol = cpos;
+    if (lidx < nleaves && b + lane < s1)
+    {
+        load_sample(P.s_rec, b + lane, cpos, cmot);
+        ccol = P.s_col[b + lane];
+    }
+    int nsurf = 0, lidx0 = 0, quad = 0, nearest = -1, result = -1, first_leaf = -1;
     float minDist = kF32Max;
     float4 acc = make_float4(0, 0, 0, 0);
-    for (int lidx = 0; lidx < nleaves; lidx++)
+    while (lidx < nleaves && result < 0)
     {
-        bool first = true;
-        const QNode node = P.nodes[leaves[lidx].node];
-        const int s0 = node.d.z, s1 = node.d.w;
-        for (int i = s0; i < s1; i++)
+        // next chunk and its loads
+        int nlidx = lidx, nb = b + 32, ns1 = s1;
+        if (nb >= s1)
         {
-            const float4 sp4 = P.s_pos[i];
-            const float4 sm = P.s_mot[i];
+            nlidx = next_leaf(lidx);
+            nb = __shfl_sync(0xffffffffu, my_s0, nlidx & 31);
+            ns1 = __shfl_sync(0xffffffffu, my_s1, nlidx & 31);
+        }
+        float4 npos = make_float4(0, 0, 0, 0), nmot = npos, ncol = npos;
+        if (nlidx < nleaves && nb + lane < ns1)
+        {
+            load_sample(P.s_rec, nb + lane, npos, nmot);
+            ncol = P.s_col[nb + lane];
+        }
+        // the current chunk
+        const int i = b + lane;
+        float dx = 0, dy = 0, dist2 = 0;
+        bool ok = false;
+        if (i < s1)
+        {
             float x, y;
-            if (sm.x != 0.0f || sm.y != 0.0f || sm.z != 0.0f)
+            if (cmot.x != 0.0f || cmot.y != 0.0f || cmot.z != 0.0f)
             {
-                const float dt = o.t - sp4.w;
-                const float Px = sp4.x * sp4.z + sm.x * dt;
-                const float Py = sp4.y * sp4.z + sm.y * dt;
-                const float Pw = (1.0f * sp4.z) + sm.z * dt;
+                const float dt = o.t - cpos.w;
+                const float Px = cpos.x * cpos.z + cmot.x * dt;
+                const float Py = cpos.y * cpos.z + cmot.y * dt;
+                const float Pw = (1.0f * cpos.z) + cmot.z * dt;
                 const float cr = rcp(Pw);
                 const float coc = P.c0 / Pw + P.c1;
                 x = Px * cr + o.u * coc;
@@ -576,73 +725,91 @@ TLFR_HD int light_query(const QParams& P, int* stack, Leaf* leaves, const Query&
             }
             else
             {
-                x = sp4.x + o.u * sm.w;
-                y = sp4.y + o.v * sm.w;
+                x = cpos.x + o.u * cmot.w;
+                y = cpos.y + o.v * cmot.w;
             }
-            const float dx = x - o.x, dy = y - o.y;
-            const float dist2 = dx * dx + dy * dy;
-            if (dist2 <= R2)
+            dx = x - o.x;
+            dy = y - o.y;
+            dist2 = dx * dx + dy * dy;
+            ok = dist2 <= R2;
+        }
+        if (__ballot_sync(0xffffffffu, ok))
+        {
+            if (first_leaf != lidx)
             {
-                if (first)
+                // first accepted sample of this leaf
+                first_leaf = lidx;
+                if (nsurf == 0)
                 {
-                    first = false;
+                    nsurf = 1;
+                    lidx0 = lidx;
+                }
+                else
+                {
+                    const QNode cur = P.nodes[leaf_node(leaves, lidx)];
                     bool same = true;
-                    for (int j = surfaceStart; j < lidx && same; ++j)
-                        same = same_surface(node, P.nodes[leaves[j].node], uvtmin, uvtmax);
-                    if (!same || nsurf == 0)
+                    for (int jb = lidx0; jb < lidx && same; jb += 32)
                     {
-                        if (nsurf == 1)
-                        {
-                            // a second surface opens: the first one is final
-                            if (quad == 0xF)
-                                goto resolved;
-                            return 1;
-                        }
-                        nsurf = 1;
-                        surfaceStart = lidx;
+                        const int j = jb + lane;
+                        const bool sj = j < lidx ? same_surface(cur, P.nodes[leaf_node(leaves, j)], uvtmin, uvtmax) : true;
+                        same = __all_sync(0xffffffffu, sj);
                     }
+                    if (!same)
+                        result = (quad == 0xF) ? 0 : 1;   // a second surface opens: the first one is final
                 }
-                quad |= 1 << (((dx >= 0 ? 1 : 4) | (dy >= 0 ? 2 : 8)) & 3);
-                const float dist = sqrtf(dist2);
-                if (dist < minDist)
+            }
+            if (result < 0)
+            {
+                quad |= __reduce_or_sync(0xffffffffu, ok ? 1 << (((dx >= 0 ? 1 : 4) | (dy >= 0 ? 2 : 8)) & 3) : 0);
+                // first strict minimum in sample order (RO.cpp:494-499)
+                const float dist = ok ? sqrtf(dist2) : __int_as_float(0x7f800000);
+                float cmin = dist;
+                for (int off = 16; off > 0; off >>= 1)
+                    cmin = minr(cmin, __shfl_xor_sync(0xffffffffu, cmin, off));
+                if (cmin < minDist)
                 {
-                    minDist = dist;
-                    nearest = i;
+                    const unsigned at = __ballot_sync(0xffffffffu, ok && dist == cmin);
+                    minDist = cmin;
+                    nearest = __shfl_sync(0xffffffffu, i, __ffs(at) - 1);
                 }
-                // tent filter over the first surface (RO.cpp:274-294); |o - r| == dist
+                // tent filter products in parallel, summed in sample order
                 const float weight = 1 - dist / R;
-                if (weight > 0)
+                const bool inc = ok && weight > 0;
+                const float4 pr = inc ? make_float4(ccol.x * weight, ccol.y * weight, ccol.z * weight, ccol.w * weight)
+                                      : make_float4(0, 0, 0, 0);
+                for (unsigned mi = __ballot_sync(0xffffffffu, inc); mi; mi &= mi - 1)
                 {
-                    const float4 c = P.s_col[i];
-                    acc.x += c.x * weight;
-                    acc.y += c.y * weight;
-                    acc.z += c.z * weight;
-                    acc.w += c.w * weight;
+                    const int src = __ffs(mi) - 1;
+                    acc.x += __shfl_sync(0xffffffffu, pr.x, src);
+                    acc.y += __shfl_sync(0xffffffffu, pr.y, src);
+                    acc.z += __shfl_sync(0xffffffffu, pr.z, src);
+                    acc.w += __shfl_sync(0xffffffffu, pr.w, src);
                 }
             }
         }
+        lidx = nlidx; b = nb; s1 = ns1;
+        cpos = npos; cmot = nmot; ccol = ncol;
     }
-    if (nsurf == 0)
-        return 1;
-resolved:
+    if (result < 0)
+        result = (nsurf == 0) ? 1 : 0;
+    if (result != 0)
+        return result;
+    const float oow = rcp(acc.w);
+    acc.x *= oow; acc.y *= oow; acc.z *= oow; acc.w *= oow;
+    if (acc.w == 0)
+        acc = P.s_col[nearest];
+    if (P.lens_filter == 1)
     {
-        const float oow = rcp(acc.w);
-        acc.x *= oow; acc.y *= oow; acc.z *= oow; acc.w *= oow;
-        if (acc.w == 0)
-            acc = P.s_col[nearest];
-        if (P.lens_filter == 1)
-        {
-            float g = gaussian(o.u, 0.5f, 0) * gaussian(o.v, 0.5f, 0);
-            acc.x *= g; acc.y *= g; acc.z *= g; acc.w *= g;
-        }
-        if (P.time_filter == 1)
-        {
-            float g = gaussian(o.t, 0.25f, 0.5f);
-            acc.x *= g; acc.y *= g; acc.z *= g; acc.w *= g;
-        }
-        out = acc;
-        return 0;
+        float g = gaussian(o.u, 0.5f, 0) * gaussian(o.v, 0.5f, 0);
+        acc.x *= g; acc.y *= g; acc.z *= g; acc.w *= g;
     }
+    if (P.time_filter == 1)
+    {
+        float g = gaussian(o.t, 0.25f, 0.5f);
+        acc.x *= g; acc.y *= g; acc.z *= g; acc.w *= g;
+    }
+    out = acc;
+    return 0;
 }
 
 __device__ __forceinline__ Query query_of(const QParams& P, long long q)
@@ -679,23 +846,57 @@ __global__ void __launch_bounds__(kBlock)
 k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
               int* __restrict__ heavy_count)
 {
-    int stack[kLStack];
-    Leaf leaves[kLLeaf];
+    __shared__ float2 sh_leaves[kLLeaf][kBlock];
+    __shared__ int sh_stack[kLStack][kBlock];
+    const int lane = threadIdx.x & 31;
+    const int wbase = threadIdx.x & ~31;
+    const Column<int> stack{ &sh_stack[0][threadIdx.x], kBlock };
     for (long long base = (long long)blockIdx.x * kBlock; base < num_queries; base += (long long)gridDim.x * kBlock)
     {
+        // each lane: traversal and leaf sort of its own output sample
         const long long q = base + threadIdx.x;
+        const bool valid = q < num_queries;
+        Query o{};
+        int nl = -2;
+        if (valid)
+        {
+            o = query_of(P, q);
+            nl = light_collect(P, stack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, o);
+        }
+        __syncwarp();
+        // the warp: the 1R scan of each lane's output sample in turn
+        int code = 2;
+        float4 col = make_float4(0, 0, 0, 0);
+        for (int j = 0; j < 32; j++)
+        {
+            const int nlj = __shfl_sync(0xffffffffu, nl, j);
+            if (nlj < 0)
+                continue;
+            Query oj;
+            oj.x = __shfl_sync(0xffffffffu, o.x, j);
+            oj.y = __shfl_sync(0xffffffffu, o.y, j);
+            oj.u = __shfl_sync(0xffffffffu, o.u, j);
+            oj.v = __shfl_sync(0xffffffffu, o.v, j);
+            oj.t = __shfl_sync(0xffffffffu, o.t, j);
+            float4 c;
+            const int r = light_scan_warp(P, Column<float2>{ &sh_leaves[0][wbase + j], kBlock }, nlj, oj, c);
+            if (lane == j)
+            {
+                code = r;
+                col = c;
+            }
+        }
+        __syncwarp();
         bool hv = false;
         int entry = 0;
-        if (q < num_queries)
+        if (valid)
         {
-            float4 c;
-            const int r = light_query(P, stack, leaves, query_of(P, q), c);
-            if (r == 0)
-                qcol[q] = c;
+            if (code == 0)
+                qcol[q] = col;
             else
             {
                 hv = true;
-                entry = (int)q | (r == 2 ? kQueueRestart : 0);
+                entry = (int)q | (code == 2 ? kQueueRestart : 0);
             }
         }
         warp_append(heavy, heavy_count, hv, entry);
@@ -739,8 +940,8 @@ __device__ __forceinline__ unsigned lanes_below(int lane) { return (1u << lane) 
 // (RO.cpp:436-454); the same operations as collect().
 __device__ __forceinline__ float reproject(const QParams& P, int i, const Query& o, float& x, float& y)
 {
-    const float4 sp4 = P.s_pos[i];
-    const float4 sm = P.s_mot[i];
+    float4 sp4, sm;
+    load_sample(P.s_rec, i, sp4, sm);
     if (sm.x != 0.0f || sm.y != 0.0f || sm.z != 0.0f)
     {
         const float dt = o.t - sp4.w;
@@ -779,8 +980,8 @@ __device__ int traverse_sorted(const QParams& P, const Query& o, float R, Leaf* 
                 if (nleaves == cap)
                     return -1;
                 const int s0 = node.d.z;
-                const float4 sp0 = P.s_pos[s0];
-                const float mvw = P.s_mot[s0].z;
+                const float4 sp0 = P.s_rec[2 * (s0)];
+                const float mvw = P.s_rec[2 * (s0) + 1].z;
                 leaves[nleaves].node = ni;
                 leaves[nleaves].key = sp0.z + (o.t - sp0.w) * mvw;
                 nleaves++;
@@ -1276,8 +1477,7 @@ QParams make_params(const Ctx& c)
 {
     QParams P;
     P.nodes = c.nodes;
-    P.s_pos = c.s_pos;
-    P.s_mot = c.s_mot;
+    P.s_rec = c.s_rec;
     P.s_col = c.s_col;
     P.pattern = c.d_pattern;
     P.M = c.out_spp;
