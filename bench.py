@@ -17,6 +17,9 @@ HBM: hierarchy build + per-output-sample query + pixel resolve.
   cpu_baseline   the reference's own CPU reconstruction (oracle/_ref, or the C
          restatement when the reference build is absent) on this host's cores:
          full hierarchy build + a band of rows, extrapolated to the frame.
+  routed the same frame and timing with the learned router on (trained first,
+         untimed, on plain-method labels of frames with seeds 100+), with its
+         PSNR and max error against the plain image.
 
 Multi-GPU: one process per GPU, each reconstructs its own frame (replicas; the
 path has no exchange step), timed with CUDA events, max over ranks.
@@ -56,6 +59,9 @@ def parse():
     ap.add_argument("--width", type=int, default=W)
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
+    ap.add_argument("--route-frames", type=int, default=2, help="router training frames (0: no routed run)")
+    ap.add_argument("--route-steps", type=int, default=600)
+    ap.add_argument("--route-threshold", type=float, default=0.8)
     return ap.parse_args()
 
 
@@ -148,6 +154,39 @@ def cpu_baseline_sample(rec, coc, rows, threads):
                   f"({band:.2f} s), extrapolated to {Hh} rows",
         "build_s": r.build_seconds, "band_s": band,
     }
+
+
+def train_router(args, device, W, H, S):
+    """Learned router trained on plain-method labels of held-out frames (seeds 100+), untimed."""
+    import numpy as np
+    import torch
+    import tlfr
+    feats, labels = [], []
+    for seed in range(100, 100 + args.route_frames):
+        rec, coc = tlfr.synth_scene(PRESET, W, H, S, seed)
+        d = torch.from_numpy(rec).cuda()
+        g = tlfr.TreeGather(None, tlfr.CameraParams(device=device), device_records=(d.data_ptr(), (W, H, S), coc))
+        f = torch.empty((H * W, 8), dtype=torch.float32, device="cuda")
+        lab = torch.empty(H * W, dtype=torch.float32, device="cuda")
+        img = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+        g.route_features(f.data_ptr())
+        g.route_labels(lab.data_ptr(), img.data_ptr(), 0.01)
+        feats.append(f)
+        labels.append(lab)
+        g.close()
+        del d
+    F = torch.cat(feats)
+    L = torch.cat(labels)
+    fh = F.cpu().numpy()
+    router = tlfr.Router(device, seed=3, mean=fh.mean(0), inv_std=1.0 / np.maximum(fh.std(0), 1e-6))
+    n = F.shape[0]
+    loss0 = router.gradient(F.data_ptr(), L.data_ptr(), n)[1]
+    t0 = time.perf_counter()
+    loss = router.train(F.data_ptr(), L.data_ptr(), n, steps=args.route_steps, batch=8192, lr=3e-3)
+    info = {"frames": args.route_frames, "seeds": [100, 100 + args.route_frames - 1], "pixels": n,
+            "label_mean": float(L.mean().item()), "label_tolerance": 0.01, "steps": args.route_steps,
+            "loss_initial": loss0, "loss_final": loss, "train_s": time.perf_counter() - t0}
+    return router, info
 
 
 def run_reference(args, rank, world):
@@ -262,6 +301,49 @@ def main():
     ms_per_step = total_ms / args.steps
     value = (world * Wd * Hd * args.steps / (total_ms / 1e3)) / 1e6
 
+    # learned routing: the same frame and timing with the router on, against the plain image
+    routed = None
+    if args.route_frames > 0:
+        plain_img = out.clone()
+        router, rinfo = train_router(args, local_rank, Wd, Hd, S)
+        tg.set_routing(router, args.route_threshold)
+        for _ in range(max(3, args.warmup)):
+            step()
+        torch.cuda.synchronize()
+        barrier()
+        r0 = torch.cuda.Event(enable_timing=True)
+        r1 = torch.cuda.Event(enable_timing=True)
+        r0.record(stream)
+        for _ in range(args.steps):
+            step()
+        r1.record(stream)
+        torch.cuda.synchronize()
+        r_ms = r0.elapsed_time(r1)
+        if dist:
+            t = torch.tensor([r_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            r_ms = float(t.item())
+        rs = tg.stats()
+        import numpy as np
+        a = out[..., :3].double()
+        b = plain_img[..., :3].double()
+        mse = float(((a - b) ** 2).mean().item())
+        prob = torch.empty(Wd * Hd, dtype=torch.float32, device="cuda")
+        feats = torch.empty((Hd * Wd, 8), dtype=torch.float32, device="cuda")
+        tg.route_features(feats.data_ptr())
+        router.predict(feats.data_ptr(), Wd * Hd, prob.data_ptr())
+        routed = {
+            "value": (world * Wd * Hd * args.steps / (r_ms / 1e3)) / 1e6, "unit": "Mpix/s",
+            "ms_per_step": r_ms / args.steps, "speedup_vs_plain": total_ms / r_ms,
+            "psnr_vs_plain_db": (10 * float(np.log10(1.0 / mse))) if mse > 0 else None,
+            "max_abs_err_vs_plain": float((a - b).abs().max().item()),
+            "fast_pixel_fraction": float((prob > args.route_threshold).float().mean().item()),
+            "threshold": args.route_threshold, "heavy_queries": rs.num_heavy_queries,
+            "light_pass_ms": rs.light_ms, "heavy_pass_ms": rs.heavy_ms, "train": rinfo,
+        }
+        tg.set_routing(None)
+        router.close()
+
     # end to end through the public API with host buffers (pinned records in,
     # RGBA image out); every rank runs it, timed by its own clock, max over ranks
     buf = tlfr.UVTSampleBuffer(records=rec, coc=coc)
@@ -309,6 +391,7 @@ def main():
                         "frac_2r": st.num_2r / st.num_output_samples,
                         "overflow_queries": st.num_overflow_queries},
         "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk,
+        "routed": routed,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(rec, coc, args.cpu_rows, os.cpu_count() or 1)

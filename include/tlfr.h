@@ -221,6 +221,50 @@ enum
 tlfr_status tlfr_synth_scene(int preset, int width, int height, int spp, unsigned long long seed,
                              float* records, float* coc_out);
 
+/* ---- learned routing (no counterpart in the reference) --------------------
+ * The router is the north-star addition: a small network predicts, per pixel,
+ * whether the fast path reproduces the plain method there; pixels above the
+ * threshold take the fast path (the plain 1R pass, which keeps the first
+ * surface when a second one opens instead of refetching at 2R; only output
+ * samples with nothing within 1R still take the full path), the rest take the
+ * plain method.  Features, labels and the
+ * network are described in temporal-lightfield-reconstruction_b200/csrc/tlfr_route.cu. */
+#define TLFR_ROUTE_FEATURES 8
+typedef struct tlfr_router tlfr_router;
+
+/* Eight features per pixel of the context's current hierarchy and records,
+ * written to d_feats (device, width*height*8 floats, row-major). */
+tlfr_status tlfr_route_features(tlfr_ctx* ctx, float* d_feats);
+/* Plain reconstruction of the current frame into d_rgba (device, RGBA float)
+ * and the per-pixel labels (device, width*height floats): 1 where the fast
+ * path reproduces the plain pixel within tol on every channel, 0 elsewhere. */
+tlfr_status tlfr_route_labels(tlfr_ctx* ctx, float tol, float* d_labels, float* d_rgba);
+/* New 8-64-64-1 network on a device, He-initialised from seed; mean8/inv_std8
+ * (host, 8 floats each, may be null) standardise the features. */
+tlfr_status tlfr_router_create(int device, void* stream, unsigned seed, const float* mean8, const float* inv_std8,
+                               tlfr_router** out);
+void        tlfr_router_destroy(tlfr_router* router);
+const char* tlfr_router_last_error(const tlfr_router* router);
+/* Number of floats of the parameter block of tlfr_router_get/set_params. */
+int         tlfr_router_num_params(void);
+/* steps Adam steps (lr; betas 0.9, 0.999) of binary cross-entropy over minibatches
+ * of batch rows drawn from the n (feature, label) rows (device pointers). */
+tlfr_status tlfr_router_train(tlfr_router* router, const float* d_feats, const float* d_labels, int n, int steps,
+                              int batch, float lr, unsigned seed, float* final_loss);
+/* Gradient of the mean cross-entropy over exactly rows 0..n-1, copied to grad
+ * (host, the trainable prefix of the parameter block), and the loss. */
+tlfr_status tlfr_router_gradient(tlfr_router* router, const float* d_feats, const float* d_labels, int n, float* grad,
+                                 float* loss);
+/* Single-surface probability of n pixels (device in, device out). */
+tlfr_status tlfr_router_predict(tlfr_router* router, const float* d_feats, long long n, float* d_prob);
+tlfr_status tlfr_router_get_params(tlfr_router* router, float* params);
+tlfr_status tlfr_router_set_params(tlfr_router* router, const float* params);
+/* Routed reconstruction: tlfr_reconstruct then computes the features, runs the
+ * network and sends pixels with probability above threshold to the fast path.
+ * router = null restores the plain method.  The router must outlive the
+ * setting, and records passed by device pointer must stay valid. */
+tlfr_status tlfr_set_routing(tlfr_ctx* ctx, tlfr_router* router, float threshold);
+
 #ifdef __cplusplus
 }
 #endif

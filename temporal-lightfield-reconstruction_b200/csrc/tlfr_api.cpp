@@ -355,7 +355,8 @@ void free_ctx_buffers(tlfr::Ctx& c)
                      c.cell_count, c.cell_start, c.cell_items, c.kd, c.kd_level, c.kd_leaves_ordered, c.perm, c.box,
                      c.sbounds, c.surface, c.pending, c.leaf_task_rank, c.ordered_n, c.ordered_prefmax, c.top,
                      c.nodes, c.node_tspan, c.s_rec, c.s_col, c.s_id, c.d_pattern, c.accum, c.qcol, c.heavy_queue, c.ovf_queue,
-                     c.ovf_scratch, c.coop_scratch, c.d_stats, c.d_out };
+                     c.ovf_scratch, c.coop_scratch, c.d_stats, c.d_out, c.route_fa, c.route_feats, c.route_prob,
+                     c.route_fast, c.route_img };
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.ev0) cudaEventDestroy(c.ev0);
@@ -423,6 +424,7 @@ tlfr_status run_build(tlfr_ctx* ctx, const float* d_rec)
     tlfr::Ctx& c = ctx->c;
     cudaEventRecord(c.ev0, c.stream);
     const long long l0 = c.launches;
+    c.cur_records = d_rec;
     tlfr_status st = tlfr::build_hierarchy(c, d_rec);
     c.last.build_launches = (double)(c.launches - l0);
     if (st != TLFR_OK)
@@ -927,6 +929,178 @@ tlfr_status tlfr_trace_queries(tlfr_ctx* ctx, const int* xyi, int n, float* rgba
             xyi[3 * k + 2] < 0 || xyi[3 * k + 2] >= c.out_spp)
             return fail(ctx, TLFR_BAD_ARG, "tlfr_trace_queries: query %d out of range", k);
     return tlfr::trace_queries(c, xyi, n, rgba, trace, stride);
+}
+
+/* ---- learned routing ------------------------------------------------------ */
+
+struct tlfr_router
+{
+    tlfr::Route r;
+};
+
+tlfr_status tlfr_route_features(tlfr_ctx* ctx, float* d_feats)
+{
+    if (!ctx || !d_feats)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_route_features: bad argument");
+    tlfr::Ctx& c = ctx->c;
+    cudaSetDevice(c.device);
+    std::string err;
+    tlfr_status st = tlfr::route_features(c, d_feats, err);
+    if (st != TLFR_OK)
+        return fail(ctx, st, "tlfr_route_features: %s", err.c_str());
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "tlfr_route_features: %s", cudaGetErrorString(e));
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_route_labels(tlfr_ctx* ctx, float tol, float* d_labels, float* d_rgba)
+{
+    if (!ctx || !d_labels || !d_rgba || !(tol >= 0.0f))
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_route_labels: bad argument");
+    tlfr::Ctx& c = ctx->c;
+    cudaSetDevice(c.device);
+    const size_t npix = (size_t)c.W * c.H;
+    if (!c.route_img)
+    {
+        cudaError_t e = cudaMalloc(&c.route_img, sizeof(float4) * npix);
+        if (e != cudaSuccess)
+            return fail(ctx, TLFR_OOM, "tlfr_route_labels: %s", cudaGetErrorString(e));
+    }
+    tlfr::Route* saved = c.router;
+    c.router = nullptr;
+    tlfr_status st = tlfr::reconstruct_frame(c, reinterpret_cast<float4*>(d_rgba), false);
+    if (st == TLFR_OK)
+    {
+        c.route_all_fast = true;
+        st = tlfr::reconstruct_frame(c, c.route_img, false);
+        c.route_all_fast = false;
+    }
+    c.router = saved;
+    if (st != TLFR_OK)
+        return fail(ctx, st, "tlfr_route_labels: %s", c.error.c_str());
+    std::string err;
+    st = tlfr::route_labels_from(c, reinterpret_cast<const float4*>(d_rgba), c.route_img, tol, d_labels, err);
+    if (st != TLFR_OK)
+        return fail(ctx, st, "tlfr_route_labels: %s", err.c_str());
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "tlfr_route_labels: %s", cudaGetErrorString(e));
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_router_create(int device, void* stream, unsigned seed, const float* mean8, const float* inv_std8,
+                               tlfr_router** out)
+{
+    if (!out)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_router_create: bad argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, TLFR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_router_create: device %d out of range", device);
+    cudaSetDevice(device);
+    tlfr_router* r = new (std::nothrow) tlfr_router;
+    if (!r)
+        return fail(nullptr, TLFR_OOM, "host allocation failed");
+    r->r.device = device;
+    r->r.stream = static_cast<cudaStream_t>(stream);
+    std::string err;
+    tlfr_status st = tlfr::route_alloc(r->r, err);
+    if (st == TLFR_OK)
+        st = tlfr::route_init(r->r, seed, mean8, inv_std8, r->r.stream, err);
+    if (st != TLFR_OK)
+    {
+        g_create_error = err;
+        tlfr::route_free(r->r);
+        delete r;
+        return st;
+    }
+    *out = r;
+    return TLFR_OK;
+}
+
+void tlfr_router_destroy(tlfr_router* r)
+{
+    if (!r)
+        return;
+    cudaSetDevice(r->r.device);
+    tlfr::route_free(r->r);
+    delete r;
+}
+
+const char* tlfr_router_last_error(const tlfr_router* r) { return r ? r->r.error.c_str() : g_create_error.c_str(); }
+
+int tlfr_router_num_params(void) { return tlfr::route_num_params(); }
+
+#define ROUTER_CALL(name, expr)                                                       \
+    do {                                                                              \
+        cudaSetDevice(r->r.device);                                                   \
+        std::string err;                                                              \
+        tlfr_status st = (expr);                                                      \
+        if (st != TLFR_OK)                                                            \
+            r->r.error = std::string(name) + ": " + err;                              \
+        return st;                                                                    \
+    } while (0)
+
+tlfr_status tlfr_router_train(tlfr_router* r, const float* d_feats, const float* d_labels, int n, int steps, int batch,
+                              float lr, unsigned seed, float* final_loss)
+{
+    if (!r || !d_feats || !d_labels || n <= 0 || steps < 0 || batch <= 0)
+        return r ? (r->r.error = "tlfr_router_train: bad argument", TLFR_BAD_ARG) : TLFR_BAD_ARG;
+    ROUTER_CALL("tlfr_router_train",
+                tlfr::route_train(r->r, d_feats, d_labels, n, steps, batch, lr, seed, final_loss, r->r.stream, err));
+}
+
+tlfr_status tlfr_router_gradient(tlfr_router* r, const float* d_feats, const float* d_labels, int n, float* grad,
+                                 float* loss)
+{
+    if (!r || !d_feats || !d_labels || n <= 0 || !grad)
+        return r ? (r->r.error = "tlfr_router_gradient: bad argument", TLFR_BAD_ARG) : TLFR_BAD_ARG;
+    ROUTER_CALL("tlfr_router_gradient",
+                tlfr::route_gradient(r->r, d_feats, d_labels, n, grad, loss, r->r.stream, err));
+}
+
+tlfr_status tlfr_router_predict(tlfr_router* r, const float* d_feats, long long n, float* d_prob)
+{
+    if (!r || !d_feats || n <= 0 || !d_prob)
+        return r ? (r->r.error = "tlfr_router_predict: bad argument", TLFR_BAD_ARG) : TLFR_BAD_ARG;
+    cudaSetDevice(r->r.device);
+    std::string err;
+    tlfr_status st = tlfr::route_predict(r->r, d_feats, n, d_prob, r->r.stream, err);
+    if (st == TLFR_OK && cudaStreamSynchronize(r->r.stream) != cudaSuccess)
+    {
+        err = cudaGetErrorString(cudaGetLastError());
+        st = TLFR_CUDA;
+    }
+    if (st != TLFR_OK)
+        r->r.error = "tlfr_router_predict: " + err;
+    return st;
+}
+
+tlfr_status tlfr_router_get_params(tlfr_router* r, float* params)
+{
+    if (!r || !params)
+        return r ? (r->r.error = "tlfr_router_get_params: bad argument", TLFR_BAD_ARG) : TLFR_BAD_ARG;
+    ROUTER_CALL("tlfr_router_get_params", tlfr::route_get_params(r->r, params, r->r.stream, err));
+}
+
+tlfr_status tlfr_router_set_params(tlfr_router* r, const float* params)
+{
+    if (!r || !params)
+        return r ? (r->r.error = "tlfr_router_set_params: bad argument", TLFR_BAD_ARG) : TLFR_BAD_ARG;
+    ROUTER_CALL("tlfr_router_set_params", tlfr::route_set_params(r->r, params, r->r.stream, err));
+}
+
+tlfr_status tlfr_set_routing(tlfr_ctx* ctx, tlfr_router* r, float threshold)
+{
+    if (!ctx || (r && !(threshold >= 0.0f && threshold < 1.0f)))
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_set_routing: bad argument");
+    if (r && r->r.device != ctx->c.device)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_set_routing: router and context are on different devices");
+    ctx->c.router = r ? &r->r : nullptr;
+    ctx->c.route_hi = threshold;
+    return TLFR_OK;
 }
 
 } // extern "C"

@@ -2,6 +2,7 @@
 // query and API translation units.
 #pragma once
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -104,6 +105,7 @@ struct Ctx
 
     // device buffers owned by the context
     float* d_records = nullptr;     // 16-float records (owned copy when created from host)
+    const float* cur_records = nullptr;   // records of the current hierarchy (read by the router)
     bool   own_records = false;
 
     // reprojected samples in input order
@@ -172,11 +174,57 @@ struct Ctx
     DevStats* d_stats = nullptr;
     float4* d_out = nullptr;        // device output when the caller passes host memory
 
+    // learned routing (tlfr_route.cu)
+    float4* route_fa = nullptr;             // per-pixel feature scratch (2 * W*H)
+    float*  route_feats = nullptr;          // W*H*8 features of the routed reconstruction
+    float*  route_prob = nullptr;           // W*H single-surface probabilities
+    unsigned char* route_fast = nullptr;    // W*H fast-path flags (first-surface 1R pass)
+    float4* route_img = nullptr;            // W*H fast-path image (router labels)
+    struct Route* router = nullptr;         // null: plain reconstruction
+    float   route_hi = 0.8f;                // probability above which a pixel takes the fast path
+    bool    route_all_fast = false;         // every pixel on the fast path (router labels)
+
     tlfr_stats last{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     cudaEvent_t evq0 = nullptr, evq1 = nullptr, evq2 = nullptr;   // around the query passes
     long long launches = 0;                         // kernels launched by this context
 };
+
+// Learned router: FP32 master parameters, Adam moments, gradient, BF16 operands.
+constexpr int kRouteFeatures = 8;
+struct Route
+{
+    float* params = nullptr;
+    float* grad = nullptr;
+    float* m = nullptr;
+    float* v = nullptr;
+    float* loss = nullptr;
+    __nv_bfloat16* half = nullptr;
+    int step = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+};
+int route_num_params();
+int route_num_trainable();
+tlfr_status route_alloc(Route& r, std::string& err);
+void route_free(Route& r);
+tlfr_status route_init(Route& r, unsigned seed, const float* mean, const float* inv_std, cudaStream_t s, std::string& err);
+tlfr_status route_set_params(Route& r, const float* host_params, cudaStream_t s, std::string& err);
+tlfr_status route_get_params(Route& r, float* host_params, cudaStream_t s, std::string& err);
+tlfr_status route_gradient(Route& r, const float* d_feats, const float* d_labels, int n, float* host_grad,
+                           float* host_loss, cudaStream_t s, std::string& err);
+tlfr_status route_train(Route& r, const float* d_feats, const float* d_labels, int n, int steps, int batch, float lr,
+                        unsigned seed, float* host_loss, cudaStream_t s, std::string& err);
+tlfr_status route_predict(Route& r, const float* d_feats, long long n, float* d_prob, cudaStream_t s, std::string& err);
+// router coarse pass: per pixel, how many of four probed output samples the
+// plain 1R pass sends to the full path (tlfr_query.cu)
+tlfr_status route_probe(Ctx& c, int* d_counts);
+constexpr int kRouteProbes = 4;
+tlfr_status route_features(Ctx& c, float* d_feats, std::string& err);
+tlfr_status route_labels_from(Ctx& c, const float4* d_plain, const float4* d_fast, float tol, float* d_labels,
+                              std::string& err);
+tlfr_status route_flags(Ctx& c, const float* d_prob, float hi, unsigned char* d_fast, std::string& err);
 
 // build: reprojection, bucketing, kd split, leaf construction, emitNodes, top.
 tlfr_status build_hierarchy(Ctx& c, const float* d_records);

@@ -53,6 +53,7 @@ struct QParams
     float c0, c1;               // refocused CoC coefficients
     float disp0;
     int   lens_filter, time_filter;
+    const unsigned char* route_fast;   // per pixel, nonzero: first-surface fast path (or null)
 };
 
 struct QStats
@@ -656,8 +657,13 @@ TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Colu
 // those leaves; when one fails the scan stops there.  All lanes call it with
 // the same arguments and get the same result: 0 with the colour in out, 1
 // when the output sample needs the 2R fetch.
+// first_surface (the learned router's fast path for pixels it marks as easy;
+// no reference counterpart): when a second surface opens, the first one is
+// taken even if its samples do not cover all four quadrants, where the
+// reference would refetch at 2R.  Output samples with nothing within 1R still
+// take the full path.
 __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, int nleaves, const Query& o,
-                               float4& out)
+                               float4& out, bool first_surface = false)
 {
     const int lane = threadIdx.x & 31;
     const float R = P.disp0;
@@ -754,8 +760,8 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
                         const bool sj = j < lidx ? same_surface(cur, P.nodes[leaf_node(leaves, j)], uvtmin, uvtmax) : true;
                         same = __all_sync(0xffffffffu, sj);
                     }
-                    if (!same)
-                        result = (quad == 0xF) ? 0 : 1;   // a second surface opens: the first one is final
+                    if (!same)   // a second surface opens: the first one is final
+                        result = (quad == 0xF || first_surface) ? 0 : 1;
                 }
             }
             if (result < 0)
@@ -842,6 +848,12 @@ __device__ __forceinline__ void warp_append(int* queue, int* count, bool pred, i
 // not known to need the 2R fetch and the full path starts it over.
 constexpr int kQueueRestart = 1 << 30;
 
+constexpr int kProbe = 4;
+
+// PROBE: the router's coarse pass.  Query k of pixel p is output sample
+// (k % kProbe) * M / kProbe (four per pixel); nothing is written but the count of
+// the pixel's probed output samples that the plain 1R pass sends to the full path.
+template <bool PROBE>
 __global__ void __launch_bounds__(kBlock)
 k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
               int* __restrict__ heavy_count)
@@ -858,11 +870,15 @@ k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* 
         const bool valid = q < num_queries;
         Query o{};
         int nl = -2;
+        const long long pix = valid ? (PROBE ? q / kProbe : q / P.M) : 0;
+        const bool fast = !PROBE && valid && P.route_fast && P.route_fast[pix];
         if (valid)
         {
-            o = query_of(P, q);
+            o = PROBE ? make_query(P, (int)(pix % P.W), (int)(pix / P.W), (int)((q % kProbe) * P.M / kProbe))
+                      : query_of(P, q);
             nl = light_collect(P, stack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, o);
         }
+        const unsigned fast_lanes = __ballot_sync(0xffffffffu, fast);
         __syncwarp();
         // the warp: the 1R scan of each lane's output sample in turn
         int code = 2;
@@ -879,7 +895,8 @@ k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* 
             oj.v = __shfl_sync(0xffffffffu, o.v, j);
             oj.t = __shfl_sync(0xffffffffu, o.t, j);
             float4 c;
-            const int r = light_scan_warp(P, Column<float2>{ &sh_leaves[0][wbase + j], kBlock }, nlj, oj, c);
+            const Column<float2> lj{ &sh_leaves[0][wbase + j], kBlock };
+            const int r = light_scan_warp(P, lj, nlj, oj, c, (fast_lanes >> j) & 1u);
             if (lane == j)
             {
                 code = r;
@@ -887,6 +904,13 @@ k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* 
             }
         }
         __syncwarp();
+        if (PROBE)
+        {
+            // heavy_count is the per-pixel count here
+            if (valid && code != 0)
+                atomicAdd(&heavy_count[pix], 1);
+            continue;
+        }
         bool hv = false;
         int entry = 0;
         if (valid)
@@ -905,7 +929,9 @@ k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* 
 
 // ---------------------------------------------------------------------------
 // Pass 2, warp-cooperative: output samples known to need the 2R fetch (the
-// light pass found fetch2R true, RO.cpp:99).  A warp takes 32 queued samples:
+// light pass found fetch2R true, RO.cpp:99), and those that outgrew the light
+// pass's capacities, which start over from the 1R fetch and its fetch2R
+// decision.  A warp takes 32 queued samples:
 //   1. each lane traverses the hierarchy at 2R for its own sample and sorts its
 //      leaves (32 independent traversals hide each other's latency);
 //   2. then, one sample at a time, the 32 lanes scan that sample's leaves
@@ -1179,20 +1205,15 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
     const int n = *queue_count;
     for (int b = warp * 32; b < n; b += nwarps * 32)
     {
-        // 1. per-lane 2R traversal and leaf sort; entries that outgrew the light
-        // pass go to the large-capacity pass
+        // 1. per-lane traversal and leaf sort: at 2R for output samples the light
+        // pass found to need it, at 1R for those that outgrew the light pass's
+        // capacities (they start over from the 1R fetch)
         const int entry = (b + lane < n) ? queue[b + lane] : -1;
         const bool restart = entry >= 0 && (entry & kQueueRestart);
-        if (restart)
-        {
-            const int slot = atomicAdd(ovf_count, 1);
-            if (slot < ovf_cap)
-                ovf_queue[slot] = entry & ~kQueueRestart;
-        }
-        const bool valid = entry >= 0 && !restart;
-        const int myq = valid ? entry : 0;
+        const bool valid = entry >= 0;
+        const int myq = valid ? (entry & ~kQueueRestart) : 0;
         Query myo = query_of(P, myq);
-        int mycount = valid ? traverse_sorted(P, myo, P.disp0 * 2, S.leaves[lane], kCLeaf) : 0;
+        int mycount = valid ? traverse_sorted(P, myo, restart ? P.disp0 : P.disp0 * 2, S.leaves[lane], kCLeaf) : 0;
         __syncwarp();
         // 2. each sample of the batch by the whole warp
         for (int j = 0; j < 32; j++)
@@ -1211,13 +1232,31 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
             o.t = __shfl_sync(0xffffffffu, myo.t, j);
             float dispersion = P.disp0;
             int nsurf = 0, total = 0;
-            if (!ovf)
+            bool fetch2R = true;
+            if (!ovf && __shfl_sync(0xffffffffu, restart, j))
+            {
+                // the 1R fetch and the fetch2R decision (RO.cpp:94-99)
+                total = coop_scan(P, o, dispersion, S.leaves[j], nl, S, nsurf);
+                ovf = total < 0;
+                if (!ovf)
+                    fetch2R = nsurf == 0 || (S.surf[0].quad != 0xF && nsurf > 1);
+                if (!ovf && fetch2R)
+                {
+                    int cnt = 0;
+                    if (lane == 0)
+                        cnt = traverse_sorted(P, o, dispersion * 2, S.leaves[j], kCLeaf);
+                    nl = __shfl_sync(0xffffffffu, cnt, 0);
+                    __syncwarp();
+                    ovf = nl < 0;
+                }
+            }
+            if (!ovf && fetch2R)
             {
                 total = coop_scan(P, o, dispersion * 2, S.leaves[j], nl, S, nsurf);
                 ovf = total < 0;
             }
             // widening when 2R found nothing (RO.cpp:110-120); lane 0 traverses
-            for (int k = 0; k < 3 && !ovf && total == 0; k++)
+            for (int k = 0; k < 3 && !ovf && fetch2R && total == 0; k++)
             {
                 dispersion *= 2.f;
                 int cnt = 0;
@@ -1241,7 +1280,7 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
                 continue;
             }
             // tiny-surface merging (RO.cpp:137-156): dst.samples += src.samples
-            for (int sidx = 0; sidx < nsurf - 1; sidx++)
+            for (int sidx = 0; fetch2R && sidx < nsurf - 1; sidx++)
             {
                 Surf src = S.surf[sidx], dst = S.surf[sidx + 1];
                 __syncwarp();
@@ -1286,7 +1325,7 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
                     nearestDist = sf.minDist;
                     nearS = sidx; nearI = sf.minIndex;
                 }
-                if (sf.minDist < 0.f || sidx == nsurf - 1)
+                if (!fetch2R || sf.minDist < 0.f || sidx == nsurf - 1)
                     found = true;
                 if (cnt >= 200)
                     found = true;
@@ -1489,6 +1528,7 @@ QParams make_params(const Ctx& c)
     P.disp0 = dispersion_for_spp(c.spp);
     P.lens_filter = c.params.lens_filter;
     P.time_filter = c.params.time_filter;
+    P.route_fast = nullptr;
     return P;
 }
 
@@ -1499,6 +1539,24 @@ constexpr int kOvSlots = 4096;
 } // namespace
 
 #define CKQ(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { c.error = std::string(#x) + ": " + cudaGetErrorString(_e); return (_e == cudaErrorMemoryAllocation) ? TLFR_OOM : TLFR_CUDA; } } while (0)
+
+tlfr_status route_probe(Ctx& c, int* d_counts)
+{
+    cudaStream_t s = c.stream;
+    const long long npix = (long long)c.W * c.H;
+    const long long nq = npix * kProbe;
+    if (nq >= kQueueRestart)
+    {
+        c.error = "route probe: frame too large";
+        return TLFR_BAD_ARG;
+    }
+    QParams P = make_params(c);
+    CKQ(cudaMemsetAsync(d_counts, 0, sizeof(int) * npix, s));
+    const int blocks = (int)std::min<long long>((nq + kBlock - 1) / kBlock, 148LL * 64);
+    TLFR_LAUNCH(c, k_query_light<true>, blocks, kBlock, s, P, nq, nullptr, nullptr, d_counts);
+    CKQ(cudaGetLastError());
+    return TLFR_OK;
+}
 
 tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
 {
@@ -1512,21 +1570,33 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
     }
     if ((size_t)nq > c.qcol_cap)
     {
-        cudaFree(c.qcol); cudaFree(c.heavy_queue);
-        c.qcol = nullptr; c.heavy_queue = nullptr; c.qcol_cap = 0;
+        // the overflow queue holds every output sample in the worst case, so no
+        // scene can exceed it
+        cudaFree(c.qcol); cudaFree(c.heavy_queue); cudaFree(c.ovf_queue);
+        c.qcol = nullptr; c.heavy_queue = nullptr; c.ovf_queue = nullptr; c.qcol_cap = 0; c.ovf_cap = 0;
         CKQ(cudaMalloc(&c.qcol, sizeof(float4) * nq));
         CKQ(cudaMalloc(&c.heavy_queue, sizeof(int) * nq));
+        CKQ(cudaMalloc(&c.ovf_queue, sizeof(int) * nq));
         c.qcol_cap = (size_t)nq;
+        c.ovf_cap = (size_t)nq;
     }
     if (!c.d_stats)
-    {
         CKQ(cudaMalloc(&c.d_stats, sizeof(DevStats) + 8 * sizeof(int)));
-        c.ovf_cap = (size_t)1 << 22;
-        CKQ(cudaMalloc(&c.ovf_queue, sizeof(int) * c.ovf_cap));
-    }
     int* counters = reinterpret_cast<int*>(c.d_stats + 1);   // [0] overflow, [1] hard, [2] heavy
     QParams P = make_params(c);
     CKQ(cudaMemsetAsync(c.d_stats, 0, sizeof(DevStats) + 8 * sizeof(int), s));
+    if ((c.router || c.route_all_fast) && !c.route_prob)
+    {
+        CKQ(cudaMalloc(&c.route_feats, sizeof(float) * kRouteFeatures * npix));
+        CKQ(cudaMalloc(&c.route_prob, sizeof(float) * npix));
+        CKQ(cudaMalloc(&c.route_fast, npix));
+    }
+    if (c.route_all_fast)
+    {
+        // every pixel on the single-surface fast path (router labels)
+        CKQ(cudaMemsetAsync(c.route_fast, 1, npix, s));
+        P.route_fast = c.route_fast;
+    }
     const int blocks = (int)std::min<long long>((nq + kBlock - 1) / kBlock, 148LL * 64);
     if (!c.evq0)
     {
@@ -1535,6 +1605,23 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
         CKQ(cudaEventCreate(&c.evq2));
     }
     CKQ(cudaEventRecord(c.evq0, s));
+    if (c.router && !c.route_all_fast && !collect_stats)
+    {
+        // learned routing: features, network, fast-path flags
+        std::string err;
+        tlfr_status rs = route_features(c, c.route_feats, err);
+        if (rs == TLFR_OK)
+            rs = route_predict(*c.router, c.route_feats, npix, c.route_prob, s, err);
+        if (rs == TLFR_OK)
+            rs = route_flags(c, c.route_prob, c.route_hi, c.route_fast, err);
+        if (rs != TLFR_OK)
+        {
+            c.error = err;
+            return rs;
+        }
+        c.launches++;
+        P.route_fast = c.route_fast;
+    }
     if (collect_stats)
     {
         TLFR_LAUNCH(c, k_query_stats, blocks, kBlock, s, P, nq, c.qcol, c.ovf_queue, counters + 0, (int)c.ovf_cap,
@@ -1549,7 +1636,7 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
             c.coop_scratch_bytes = sizeof(CoopScratch) * coop_blocks * kCWarps;
             CKQ(cudaMalloc(&c.coop_scratch, c.coop_scratch_bytes));
         }
-        TLFR_LAUNCH(c, k_query_light, blocks, kBlock, s, P, nq, c.qcol, c.heavy_queue, counters + 2);
+        TLFR_LAUNCH(c, k_query_light<false>, blocks, kBlock, s, P, nq, c.qcol, c.heavy_queue, counters + 2);
         CKQ(cudaEventRecord(c.evq1, s));
         TLFR_LAUNCH(c, k_query_coop, coop_blocks, kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol,
                     c.ovf_queue, counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(c.coop_scratch));

@@ -107,6 +107,19 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_query_samples_noalloc": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
         "tlfr_synth_scene": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_ulonglong, _FP, _FP]),
+        "tlfr_route_features": (ctypes.c_int, [_VP, _VP]),
+        "tlfr_route_labels": (ctypes.c_int, [_VP, ctypes.c_float, _VP, _VP]),
+        "tlfr_router_create": (ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_uint, _FP, _FP, ctypes.POINTER(_VP)]),
+        "tlfr_router_destroy": (None, [_VP]),
+        "tlfr_router_last_error": (ctypes.c_char_p, [_VP]),
+        "tlfr_router_num_params": (ctypes.c_int, []),
+        "tlfr_router_train": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                             ctypes.c_uint, _FP]),
+        "tlfr_router_gradient": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, _FP, _FP]),
+        "tlfr_router_predict": (ctypes.c_int, [_VP, _VP, ctypes.c_longlong, _VP]),
+        "tlfr_router_get_params": (ctypes.c_int, [_VP, _FP]),
+        "tlfr_router_set_params": (ctypes.c_int, [_VP, _FP]),
+        "tlfr_set_routing": (ctypes.c_int, [_VP, _VP, ctypes.c_float]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -307,9 +320,90 @@ class TreeGather:
         _check(load_library().tlfr_trace_queries(self._h, _i32p(q), n, _f32p(rgba), _i32p(trace), stride), self._h)
         return rgba, trace
 
+    def route_features(self, d_feats: int):
+        """Eight routing features per pixel into device memory (W*H*8 floats)."""
+        _check(load_library().tlfr_route_features(self._h, _VP(d_feats)), self._h)
+
+    def route_labels(self, d_labels: int, d_rgba: int, tol: float = 0.01):
+        """Plain reconstruction into d_rgba plus every pixel's label (fast path within tol of it)."""
+        _check(load_library().tlfr_route_labels(self._h, tol, _VP(d_labels), _VP(d_rgba)), self._h)
+
+    def set_routing(self, router: Optional["Router"], threshold: float = 0.8):
+        """Learned routing on (router) or off (None) for the following reconstructions."""
+        _check(load_library().tlfr_set_routing(self._h, router.handle if router else None, threshold), self._h)
+        self._router = router
+
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.tlfr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Router:
+    """The learned single-surface router (8-64-64-1 MLP on the tensor cores)."""
+
+    NUM_FEATURES = 8
+
+    def __init__(self, device: int = 0, seed: int = 1, mean=None, inv_std=None, stream: int = 0):
+        lib = load_library()
+        h = _VP()
+        m = np.ascontiguousarray(mean, np.float32) if mean is not None else None
+        s = np.ascontiguousarray(inv_std, np.float32) if inv_std is not None else None
+        st = lib.tlfr_router_create(device, _VP(stream), seed, _f32p(m) if m is not None else None,
+                                    _f32p(s) if s is not None else None, ctypes.byref(h))
+        if st != 0:
+            raise TlfrError(st, (lib.tlfr_router_last_error(None) or b"").decode())
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _ok(self, st):
+        if st != 0:
+            raise TlfrError(st, (load_library().tlfr_router_last_error(self._h) or b"").decode())
+
+    def train(self, d_feats: int, d_labels: int, n: int, steps: int, batch: int = 8192, lr: float = 2e-3,
+              seed: int = 7) -> float:
+        loss = ctypes.c_float()
+        self._ok(load_library().tlfr_router_train(self._h, _VP(d_feats), _VP(d_labels), n, steps, batch, lr, seed,
+                                                  ctypes.byref(loss)))
+        return loss.value
+
+    def gradient(self, d_feats: int, d_labels: int, n: int):
+        g = np.zeros(self.num_params(), np.float32)
+        loss = ctypes.c_float()
+        self._ok(load_library().tlfr_router_gradient(self._h, _VP(d_feats), _VP(d_labels), n, _f32p(g),
+                                                     ctypes.byref(loss)))
+        return g[:self.num_trainable()], loss.value
+
+    def predict(self, d_feats: int, n: int, d_prob: int):
+        self._ok(load_library().tlfr_router_predict(self._h, _VP(d_feats), n, _VP(d_prob)))
+
+    @staticmethod
+    def num_params() -> int:
+        return load_library().tlfr_router_num_params()
+
+    @staticmethod
+    def num_trainable() -> int:
+        return Router.num_params() - 2 * Router.NUM_FEATURES
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.num_params(), np.float32)
+        self._ok(load_library().tlfr_router_get_params(self._h, _f32p(p)))
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.num_params()
+        self._ok(load_library().tlfr_router_set_params(self._h, _f32p(p)))
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tlfr_router_destroy(self._h)
             self._h = None
 
     def __del__(self):
