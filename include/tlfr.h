@@ -265,6 +265,29 @@ tlfr_status tlfr_router_set_params(tlfr_router* router, const float* params);
  * setting, and records passed by device pointer must stay valid. */
 tlfr_status tlfr_set_routing(tlfr_ctx* ctx, tlfr_router* router, float threshold);
 
+/* ---- batches -----------------------------------------------------------------
+ * Many built contexts (sample buffers of any resolution and spp) reconstructed
+ * as one CUDA graph replayed on one stream: each frame's router (if set),
+ * light pass, cooperative full-path pass, large-capacity pass and pixel resolve,
+ * with no host synchronisation inside.  With autotune, each frame's light-pass
+ * grid (resident blocks per SM) is chosen by timing candidates at creation.
+ * Replaces the reference's per-frame reconstruct loop of the animation/export
+ * paths (reconstruction_app/App.cpp:616-694).  The graph holds the contexts'
+ * buffers as they are at creation: after rebuilding a context with records of
+ * another size, create the batch again.  Outputs are device RGBA float images. */
+typedef struct tlfr_batch tlfr_batch;
+tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba, void* stream, int autotune,
+                              tlfr_batch** out);
+/* Replays the batch on its stream (asynchronous). */
+tlfr_status tlfr_batch_run(tlfr_batch* batch);
+/* Waits for the last run; device time in ms (optional); TLFR_OVERFLOW when an
+ * output sample exceeded every capacity. */
+tlfr_status tlfr_batch_sync(tlfr_batch* batch, double* ms);
+/* The light-pass grid chosen for each frame (n entries). */
+tlfr_status tlfr_batch_info(const tlfr_batch* batch, int* light_blocks);
+const char* tlfr_batch_last_error(const tlfr_batch* batch);
+void        tlfr_batch_destroy(tlfr_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

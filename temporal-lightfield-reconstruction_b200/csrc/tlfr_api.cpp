@@ -1103,4 +1103,211 @@ tlfr_status tlfr_set_routing(tlfr_ctx* ctx, tlfr_router* r, float threshold)
     return TLFR_OK;
 }
 
+/* ---- batches of frames (one CUDA graph) ------------------------------------ */
+
+struct tlfr_batch
+{
+    std::vector<tlfr_ctx*> ctx;
+    std::vector<float*> out;
+    std::vector<int> light_blocks;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string error;
+};
+
+static tlfr_status batch_fail(tlfr_batch* b, tlfr_status st, const std::string& msg)
+{
+    if (b)
+        b->error = msg;
+    else
+        g_create_error = msg;
+    return st;
+}
+
+static void batch_free(tlfr_batch* b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba, void* stream, int autotune,
+                              tlfr_batch** out)
+{
+    if (!ctxs || !d_rgba || n <= 0 || !out)
+        return batch_fail(nullptr, TLFR_BAD_ARG, "tlfr_batch_create: bad argument");
+    for (int i = 0; i < n; i++)
+        if (!ctxs[i] || !d_rgba[i])
+            return batch_fail(nullptr, TLFR_BAD_ARG, "tlfr_batch_create: null context or output " + std::to_string(i));
+    const int dev = ctxs[0]->c.device;
+    for (int i = 1; i < n; i++)
+        if (ctxs[i]->c.device != dev)
+            return batch_fail(nullptr, TLFR_BAD_ARG, "tlfr_batch_create: contexts on different devices");
+    cudaSetDevice(dev);
+    tlfr_batch* b = new (std::nothrow) tlfr_batch;
+    if (!b)
+        return batch_fail(nullptr, TLFR_OOM, "host allocation failed");
+    b->device = dev;
+    b->ctx.assign(ctxs, ctxs + n);
+    b->out.assign(d_rgba, d_rgba + n);
+    b->stream = static_cast<cudaStream_t>(stream);
+    if (!b->stream)
+    {
+        if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        {
+            batch_free(b);
+            return batch_fail(nullptr, TLFR_CUDA, "tlfr_batch_create: stream creation failed");
+        }
+        b->own_stream = true;
+    }
+    auto cuda_fail = [&](const char* what, cudaError_t e) {
+        const std::string m = std::string("tlfr_batch_create: ") + what + ": " + cudaGetErrorString(e);
+        batch_free(b);
+        return batch_fail(nullptr, TLFR_CUDA, m);
+    };
+    // buffers, then the light pass's grid per frame, then one eager run (lazy
+    // scratch of the router), then the capture
+    for (int i = 0; i < n; i++)
+    {
+        tlfr::Ctx& c = b->ctx[i]->c;
+        tlfr_status st = tlfr::frame_prepare(c);
+        if (st != TLFR_OK)
+        {
+            const std::string m = "tlfr_batch_create: frame " + std::to_string(i) + ": " + c.error;
+            batch_free(b);
+            return batch_fail(nullptr, st, m);
+        }
+        int best = tlfr::light_default_blocks(c);
+        if (autotune)
+        {
+            // persistent grids of k resident 128-thread blocks per SM, k = 2..32
+            const int cap = best;
+            float best_ms = 1e30f;
+            for (int k : { 2, 4, 8, 16, 32 })
+            {
+                const int blocks = std::min(cap, 148 * k);
+                float ms = 0;
+                st = tlfr::light_trial(c, b->stream, blocks, &ms);
+                if (st != TLFR_OK)
+                {
+                    const std::string m = "tlfr_batch_create: autotune: " + c.error;
+                    batch_free(b);
+                    return batch_fail(nullptr, st, m);
+                }
+                if (ms < best_ms)
+                {
+                    best_ms = ms;
+                    best = blocks;
+                }
+            }
+        }
+        b->light_blocks.push_back(best);
+    }
+    for (int pass = 0; pass < 2; pass++)
+    {
+        cudaError_t e = cudaSuccess;
+        if (pass == 1 && (e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+            return cuda_fail("cudaStreamBeginCapture", e);
+        for (int i = 0; i < n; i++)
+        {
+            tlfr::Ctx& c = b->ctx[i]->c;
+            tlfr_status st = tlfr::frame_enqueue(c, reinterpret_cast<float4*>(b->out[i]), b->stream, b->light_blocks[i]);
+            if (st != TLFR_OK)
+            {
+                if (pass == 1)
+                {
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(b->stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                }
+                const std::string m = "tlfr_batch_create: frame " + std::to_string(i) + ": " + c.error;
+                batch_free(b);
+                return batch_fail(nullptr, st, m);
+            }
+        }
+        if (pass == 0 && (e = cudaStreamSynchronize(b->stream)) != cudaSuccess)
+            return cuda_fail("warm-up run", e);
+        if (pass == 1)
+        {
+            if ((e = cudaStreamEndCapture(b->stream, &b->graph)) != cudaSuccess)
+                return cuda_fail("cudaStreamEndCapture", e);
+            if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess)
+                return cuda_fail("cudaGraphInstantiate", e);
+        }
+    }
+    if (cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        return cuda_fail("cudaEventCreate", cudaGetLastError());
+    *out = b;
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_batch_run(tlfr_batch* b)
+{
+    if (!b)
+        return TLFR_BAD_ARG;
+    cudaSetDevice(b->device);
+    cudaError_t e = cudaEventRecord(b->ev0, b->stream);
+    if (e == cudaSuccess)
+        e = cudaGraphLaunch(b->exec, b->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b->ev1, b->stream);
+    if (e != cudaSuccess)
+        return batch_fail(b, TLFR_CUDA, std::string("tlfr_batch_run: ") + cudaGetErrorString(e));
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_batch_sync(tlfr_batch* b, double* ms)
+{
+    if (!b)
+        return TLFR_BAD_ARG;
+    cudaSetDevice(b->device);
+    cudaError_t e = cudaEventSynchronize(b->ev1);
+    if (e != cudaSuccess)
+        return batch_fail(b, TLFR_CUDA, std::string("tlfr_batch_sync: ") + cudaGetErrorString(e));
+    if (ms)
+    {
+        float f = 0;
+        cudaEventElapsedTime(&f, b->ev0, b->ev1);
+        *ms = f;
+    }
+    for (size_t i = 0; i < b->ctx.size(); i++)
+    {
+        int hard = 0;
+        if (tlfr::frame_hard_failures(b->ctx[i]->c, b->stream, &hard) != TLFR_OK)
+            return batch_fail(b, TLFR_CUDA, "tlfr_batch_sync: " + b->ctx[i]->c.error);
+        if (hard > 0)
+            return batch_fail(b, TLFR_OVERFLOW, "tlfr_batch_sync: frame " + std::to_string(i) +
+                                                    ": a query exceeded the largest supported capacity");
+    }
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_batch_info(const tlfr_batch* b, int* light_blocks)
+{
+    if (!b || !light_blocks)
+        return TLFR_BAD_ARG;
+    for (size_t i = 0; i < b->light_blocks.size(); i++)
+        light_blocks[i] = b->light_blocks[i];
+    return TLFR_OK;
+}
+
+const char* tlfr_batch_last_error(const tlfr_batch* b) { return b ? b->error.c_str() : g_create_error.c_str(); }
+
+void tlfr_batch_destroy(tlfr_batch* b)
+{
+    if (!b)
+        return;
+    cudaSetDevice(b->device);
+    if (b->stream)
+        cudaStreamSynchronize(b->stream);
+    batch_free(b);
+}
+
 } // extern "C"

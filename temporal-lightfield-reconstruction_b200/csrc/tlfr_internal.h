@@ -230,6 +230,12 @@ tlfr_status route_flags(Ctx& c, const float* d_prob, float hi, unsigned char* d_
 tlfr_status build_hierarchy(Ctx& c, const float* d_records);
 // query: all output samples of the frame into rgba (device pointer).
 tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats);
+// the same with no host synchronisation (batches, CUDA graph capture)
+tlfr_status frame_prepare(Ctx& c);
+tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_blocks);
+tlfr_status frame_hard_failures(Ctx& c, cudaStream_t s, int* hard);
+tlfr_status light_trial(Ctx& c, cudaStream_t s, int light_blocks, float* ms);
+int light_default_blocks(const Ctx& c);
 tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h_trace, int stride);
 // output samples through the full path with working storage in a fixed device array
 tlfr_status query_samples_noalloc(Ctx& c, const int* d_xyi, int n, float* d_rgba, int* d_overflow);

@@ -1429,10 +1429,11 @@ k_query_stats(QParams P, long long num_queries, float4* __restrict__ qcol, int* 
 // Pass 3: large capacities for queries that overflowed pass 2 (or the
 // statistics pass).  Each thread slot owns a fixed region of the arena.
 __global__ void __launch_bounds__(64)
-k_query_overflow(QParams P, const int* __restrict__ queue, int count, float4* __restrict__ qcol, char* arena,
-                 size_t slot_bytes, int num_slots, int stack_cap, int leaf_cap, int rs_cap, int surf_cap,
-                 int* hard_fail, DevStats* ds, int stats)
+k_query_overflow(QParams P, const int* __restrict__ queue, const int* __restrict__ count_ptr, int cap,
+                 float4* __restrict__ qcol, char* arena, size_t slot_bytes, int num_slots, int stack_cap, int leaf_cap,
+                 int rs_cap, int surf_cap, int* hard_fail, DevStats* ds, int stats)
 {
+    const int count = min(*count_ptr, cap);
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     QStats st{};
     if (slot < num_slots)
@@ -1558,6 +1559,129 @@ tlfr_status route_probe(Ctx& c, int* d_counts)
     return TLFR_OK;
 }
 
+// Every buffer a frame's reconstruction uses, allocated ahead (a captured
+// frame may not allocate).
+tlfr_status frame_prepare(Ctx& c)
+{
+    const long long npix = (long long)c.W * c.H;
+    const long long nq = npix * c.out_spp;
+    if (nq >= kQueueRestart)
+    {
+        c.error = "more than 2^30 output samples in one frame";
+        return TLFR_BAD_ARG;
+    }
+    if ((size_t)nq > c.qcol_cap)
+    {
+        cudaFree(c.qcol); cudaFree(c.heavy_queue); cudaFree(c.ovf_queue);
+        c.qcol = nullptr; c.heavy_queue = nullptr; c.ovf_queue = nullptr; c.qcol_cap = 0; c.ovf_cap = 0;
+        CKQ(cudaMalloc(&c.qcol, sizeof(float4) * nq));
+        CKQ(cudaMalloc(&c.heavy_queue, sizeof(int) * nq));
+        CKQ(cudaMalloc(&c.ovf_queue, sizeof(int) * nq));
+        c.qcol_cap = (size_t)nq;
+        c.ovf_cap = (size_t)nq;
+    }
+    if (!c.d_stats)
+        CKQ(cudaMalloc(&c.d_stats, sizeof(DevStats) + 8 * sizeof(int)));
+    if (!c.coop_scratch)
+    {
+        c.coop_scratch_bytes = sizeof(CoopScratch) * 148 * 4 * kCWarps;
+        CKQ(cudaMalloc(&c.coop_scratch, c.coop_scratch_bytes));
+    }
+    if (!c.ovf_scratch)
+    {
+        c.ovf_scratch_bytes = slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf) * kOvSlots;
+        CKQ(cudaMalloc(&c.ovf_scratch, c.ovf_scratch_bytes));
+    }
+    if (c.router && !c.route_prob)
+    {
+        CKQ(cudaMalloc(&c.route_feats, sizeof(float) * kRouteFeatures * npix));
+        CKQ(cudaMalloc(&c.route_prob, sizeof(float) * npix));
+        CKQ(cudaMalloc(&c.route_fast, npix));
+    }
+    return TLFR_OK;
+}
+
+int light_default_blocks(const Ctx& c)
+{
+    const long long nq = (long long)c.W * c.H * c.out_spp;
+    return (int)std::min<long long>((nq + kBlock - 1) / kBlock, 148LL * 64);
+}
+
+// One frame's reconstruction issued on stream s with no host synchronisation:
+// router (when set), light pass on light_blocks blocks, cooperative pass,
+// large-capacity pass (its count read on the device), pixel resolve.  Requires
+// frame_prepare() and, with a router, one earlier reconstruction (the router's
+// feature scratch).  Capacity failures are counted on the device
+// (frame_hard_failures).
+tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_blocks)
+{
+    const long long npix = (long long)c.W * c.H;
+    const long long nq = npix * c.out_spp;
+    int* counters = reinterpret_cast<int*>(c.d_stats + 1);
+    QParams P = make_params(c);
+    cudaStream_t saved = c.stream;
+    c.stream = s;
+    CKQ(cudaMemsetAsync(c.d_stats, 0, sizeof(DevStats) + 8 * sizeof(int), s));
+    if (c.router)
+    {
+        std::string err;
+        tlfr_status rs = route_features(c, c.route_feats, err);
+        if (rs == TLFR_OK)
+            rs = route_predict(*c.router, c.route_feats, npix, c.route_prob, s, err);
+        if (rs == TLFR_OK)
+            rs = route_flags(c, c.route_prob, c.route_hi, c.route_fast, err);
+        if (rs != TLFR_OK)
+        {
+            c.stream = saved;
+            c.error = err;
+            return rs;
+        }
+        c.launches++;
+        P.route_fast = c.route_fast;
+    }
+    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, nq, c.qcol, c.heavy_queue, counters + 2);
+    TLFR_LAUNCH(c, k_query_coop, 148 * 4, kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol, c.ovf_queue,
+                counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(c.coop_scratch));
+    TLFR_LAUNCH(c, k_query_overflow, kOvSlots / 64, 64, s, P, c.ovf_queue, counters + 0, (int)c.ovf_cap, c.qcol,
+                (char*)c.ovf_scratch, slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf), kOvSlots, kOvStack, kOvLeaf,
+                kOvRs, kOvSurf, counters + 1, c.d_stats, 0);
+    TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, 148LL * 32), 128, s, c.qcol, c.out_spp,
+                d_rgba, npix);
+    c.stream = saved;
+    CKQ(cudaGetLastError());
+    return TLFR_OK;
+}
+
+// Output samples of the last enqueued frame that exceeded every capacity.
+tlfr_status frame_hard_failures(Ctx& c, cudaStream_t s, int* hard)
+{
+    int* counters = reinterpret_cast<int*>(c.d_stats + 1);
+    CKQ(cudaMemcpyAsync(hard, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CKQ(cudaStreamSynchronize(s));
+    return TLFR_OK;
+}
+
+// Device time of the light pass alone with light_blocks blocks (autotuning).
+tlfr_status light_trial(Ctx& c, cudaStream_t s, int light_blocks, float* ms)
+{
+    const long long nq = (long long)c.W * c.H * c.out_spp;
+    int* counters = reinterpret_cast<int*>(c.d_stats + 1);
+    QParams P = make_params(c);
+    cudaEvent_t e0, e1;
+    CKQ(cudaEventCreate(&e0));
+    CKQ(cudaEventCreate(&e1));
+    CKQ(cudaMemsetAsync(counters, 0, 8 * sizeof(int), s));
+    CKQ(cudaEventRecord(e0, s));
+    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, nq, c.qcol, c.heavy_queue, counters + 2);
+    CKQ(cudaEventRecord(e1, s));
+    CKQ(cudaEventSynchronize(e1));
+    CKQ(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CKQ(cudaGetLastError());
+    return TLFR_OK;
+}
+
 tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
 {
     cudaStream_t s = c.stream;
@@ -1663,7 +1787,8 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
             CKQ(cudaMalloc(&c.ovf_scratch, c.ovf_scratch_bytes));
         }
         const int slots = std::min(kOvSlots, novf);
-        TLFR_LAUNCH(c, k_query_overflow, (slots + 63) / 64, 64, s, P, c.ovf_queue, novf, c.qcol, (char*)c.ovf_scratch,
+        TLFR_LAUNCH(c, k_query_overflow, (slots + 63) / 64, 64, s, P, c.ovf_queue, counters + 0, (int)c.ovf_cap,
+                    c.qcol, (char*)c.ovf_scratch,
                     sb, slots, kOvStack, kOvLeaf, kOvRs, kOvSurf, counters + 1, c.d_stats, collect_stats ? 1 : 0);
         CKQ(cudaGetLastError());
         CKQ(cudaMemcpyAsync(&hard, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -120,6 +120,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_router_get_params": (ctypes.c_int, [_VP, _FP]),
         "tlfr_router_set_params": (ctypes.c_int, [_VP, _FP]),
         "tlfr_set_routing": (ctypes.c_int, [_VP, _VP, ctypes.c_float]),
+        "tlfr_batch_create": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int, ctypes.POINTER(_VP), _VP,
+                                             ctypes.c_int, ctypes.POINTER(_VP)]),
+        "tlfr_batch_run": (ctypes.c_int, [_VP]),
+        "tlfr_batch_sync": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double)]),
+        "tlfr_batch_info": (ctypes.c_int, [_VP, _IP]),
+        "tlfr_batch_last_error": (ctypes.c_char_p, [_VP]),
+        "tlfr_batch_destroy": (None, [_VP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -404,6 +411,48 @@ class Router:
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.tlfr_router_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Batch:
+    """Several built TreeGather contexts reconstructed as one CUDA graph (tlfr_batch_*)."""
+
+    def __init__(self, trees: Sequence["TreeGather"], outputs: Sequence[int], stream: int = 0, autotune: bool = True):
+        lib = load_library()
+        n = len(trees)
+        self._trees = list(trees)
+        hs = (_VP * n)(*[t.handle for t in trees])
+        outs = (_VP * n)(*[_VP(p) for p in outputs])
+        h = _VP()
+        st = lib.tlfr_batch_create(hs, n, outs, _VP(stream), 1 if autotune else 0, ctypes.byref(h))
+        if st != 0:
+            raise TlfrError(st, (lib.tlfr_batch_last_error(None) or b"").decode())
+        self._h = h
+        self.n = n
+
+    def _ok(self, st):
+        if st != 0:
+            raise TlfrError(st, (load_library().tlfr_batch_last_error(self._h) or b"").decode())
+
+    def run(self):
+        self._ok(load_library().tlfr_batch_run(self._h))
+
+    def sync(self) -> float:
+        ms = ctypes.c_double()
+        self._ok(load_library().tlfr_batch_sync(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def light_blocks(self):
+        b = np.zeros(self.n, np.int32)
+        self._ok(load_library().tlfr_batch_info(self._h, _i32p(b)))
+        return b
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tlfr_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):
