@@ -20,6 +20,9 @@ HBM: hierarchy build + per-output-sample query + pixel resolve.
   routed the same frame and timing with the learned router on (trained first,
          untimed, on plain-method labels of frames with seeds 100+), with its
          PSNR and max error against the plain image.
+  batch  uneven sample buffers (resolution and spp drawn per buffer) built as
+         contexts and reconstructed as one CUDA graph per run, router on;
+         Mpix/s over all buffers.  --batch-scale 1 is the full-size mix.
 
 Multi-GPU: one process per GPU, each reconstructs its own frame (replicas; the
 path has no exchange step), timed with CUDA events, max over ranks.
@@ -62,6 +65,8 @@ def parse():
     ap.add_argument("--route-frames", type=int, default=2, help="router training frames (0: no routed run)")
     ap.add_argument("--route-steps", type=int, default=600)
     ap.add_argument("--route-threshold", type=float, default=0.8)
+    ap.add_argument("--batch-frames", type=int, default=48, help="uneven-buffer batch size (0: no batch run)")
+    ap.add_argument("--batch-scale", type=int, default=4, help="linear downscale of the batch's resolutions")
     return ap.parse_args()
 
 
@@ -187,6 +192,59 @@ def train_router(args, device, W, H, S):
             "label_mean": float(L.mean().item()), "label_tolerance": 0.01, "steps": args.route_steps,
             "loss_initial": loss0, "loss_final": loss, "train_s": time.perf_counter() - t0}
     return router, info
+
+
+BATCH_RES = [(320, 240), (640, 480), (962, 543), (1280, 720), (1920, 1080)]
+BATCH_SPP = [1, 2, 4, 8, 16]
+
+
+def run_batch(args, device, router, steps, warmup):
+    """Uneven buffers (resolution and spp drawn per frame, the 64-rectangle scene
+    generator per seed) reconstructed as one CUDA graph, router on."""
+    import numpy as np
+    import torch
+    import tlfr
+    rng = np.random.default_rng(4)
+    trees, outs, recs, pix = [], [], [], 0
+    shapes = []
+    for k in range(args.batch_frames):
+        Wr, Hr = BATCH_RES[rng.integers(len(BATCH_RES))]
+        Wb, Hb = max(8, Wr // args.batch_scale), max(8, Hr // args.batch_scale)
+        Sb = int(BATCH_SPP[rng.integers(len(BATCH_SPP))])
+        rec, coc = tlfr.synth_scene(tlfr.SCENE_CARDS, Wb, Hb, Sb, 1000 + k)
+        d = torch.from_numpy(rec).cuda()
+        g = tlfr.TreeGather(None, tlfr.CameraParams(device=device), device_records=(d.data_ptr(), (Wb, Hb, Sb), coc))
+        if router is not None:
+            g.set_routing(router, args.route_threshold)
+        recs.append(d)
+        trees.append(g)
+        outs.append(torch.empty((Hb, Wb, 4), dtype=torch.float32, device="cuda"))
+        shapes.append((Wb, Hb, Sb))
+        pix += Wb * Hb
+    t0 = time.perf_counter()
+    batch = tlfr.Batch(trees, [o.data_ptr() for o in outs], autotune=True)
+    create_s = time.perf_counter() - t0
+    for _ in range(warmup):
+        batch.run()
+        batch.sync()
+    ms = []
+    for _ in range(steps):
+        batch.run()
+        ms.append(batch.sync())
+    blocks = batch.light_blocks()
+    batch.close()
+    for g in trees:
+        g.close()
+    t = statistics.median(ms)
+    return {
+        "config": f"{args.batch_frames} buffers, resolutions drawn from {BATCH_RES} divided by {args.batch_scale}, "
+                  f"spp drawn from {BATCH_SPP}, 64-rectangle scene per seed, 128 output samples/px, "
+                  f"router {'on' if router is not None else 'off'}",
+        "frames": args.batch_frames, "pixels": pix, "output_samples": pix * 128,
+        "value": pix / (t / 1e3) / 1e6, "unit": "Mpix/s", "ms_per_run": t, "runs": steps,
+        "create_s": create_s, "light_grid_blocks": sorted(set(int(b) for b in blocks)),
+        "launch": "one CUDA graph per run",
+    }
 
 
 def run_reference(args, rank, world):
@@ -342,6 +400,13 @@ def main():
             "light_pass_ms": rs.light_ms, "heavy_pass_ms": rs.heavy_ms, "train": rinfo,
         }
         tg.set_routing(None)
+
+    # uneven-buffer batch (one CUDA graph), learned routing on
+    batch = None
+    if args.batch_frames > 0:
+        batch = run_batch(args, local_rank, router if args.route_frames > 0 else None, max(1, min(args.steps, 5)),
+                          max(1, min(args.warmup, 3)))
+    if args.route_frames > 0:
         router.close()
 
     # end to end through the public API with host buffers (pinned records in,
@@ -391,7 +456,7 @@ def main():
                         "frac_2r": st.num_2r / st.num_output_samples,
                         "overflow_queries": st.num_overflow_queries},
         "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk,
-        "routed": routed,
+        "routed": routed, "batch": batch,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(rec, coc, args.cpu_rows, os.cpu_count() or 1)

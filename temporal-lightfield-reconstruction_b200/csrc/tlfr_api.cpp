@@ -1116,6 +1116,8 @@ struct tlfr_batch
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void* coop_scratch = nullptr;   // working storage of the full-path passes, shared by the
+    void* ovf_scratch = nullptr;    // batch's frames (they run one after another on its stream)
     std::string error;
 };
 
@@ -1135,6 +1137,8 @@ static void batch_free(tlfr_batch* b)
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    if (b->coop_scratch) cudaFree(b->coop_scratch);
+    if (b->ovf_scratch) cudaFree(b->ovf_scratch);
     delete b;
 }
 
@@ -1172,12 +1176,22 @@ tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba
         batch_free(b);
         return batch_fail(nullptr, TLFR_CUDA, m);
     };
-    // buffers, then the light pass's grid per frame, then one eager run (lazy
-    // scratch of the router), then the capture
+    // shared working storage, each frame's buffers, the light pass's grid per
+    // frame, one eager run (lazy scratch of the router), then the capture
+    {
+        cudaError_t e = cudaMalloc(&b->coop_scratch, tlfr::coop_scratch_bytes());
+        if (e == cudaSuccess)
+            e = cudaMalloc(&b->ovf_scratch, tlfr::overflow_scratch_bytes());
+        if (e != cudaSuccess)
+        {
+            batch_free(b);
+            return batch_fail(nullptr, TLFR_OOM, std::string("tlfr_batch_create: scratch: ") + cudaGetErrorString(e));
+        }
+    }
     for (int i = 0; i < n; i++)
     {
         tlfr::Ctx& c = b->ctx[i]->c;
-        tlfr_status st = tlfr::frame_prepare(c);
+        tlfr_status st = tlfr::frame_prepare(c, false);
         if (st != TLFR_OK)
         {
             const std::string m = "tlfr_batch_create: frame " + std::to_string(i) + ": " + c.error;
@@ -1218,7 +1232,8 @@ tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba
         for (int i = 0; i < n; i++)
         {
             tlfr::Ctx& c = b->ctx[i]->c;
-            tlfr_status st = tlfr::frame_enqueue(c, reinterpret_cast<float4*>(b->out[i]), b->stream, b->light_blocks[i]);
+            tlfr_status st = tlfr::frame_enqueue(c, reinterpret_cast<float4*>(b->out[i]), b->stream, b->light_blocks[i],
+                                                 b->coop_scratch, b->ovf_scratch);
             if (st != TLFR_OK)
             {
                 if (pass == 1)

@@ -231,8 +231,14 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records);
 // query: all output samples of the frame into rgba (device pointer).
 tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats);
 // the same with no host synchronisation (batches, CUDA graph capture)
-tlfr_status frame_prepare(Ctx& c);
-tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_blocks);
+// own_scratch: allocate the context's own working storage of the full-path
+// passes; batches pass one shared set to frame_enqueue instead (null: the
+// context's own)
+tlfr_status frame_prepare(Ctx& c, bool own_scratch);
+tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_blocks, void* coop_scratch,
+                          void* ovf_scratch);
+size_t coop_scratch_bytes();
+size_t overflow_scratch_bytes();
 tlfr_status frame_hard_failures(Ctx& c, cudaStream_t s, int* hard);
 tlfr_status light_trial(Ctx& c, cudaStream_t s, int light_blocks, float* ms);
 int light_default_blocks(const Ctx& c);
