@@ -562,9 +562,10 @@ struct LLeafSort
 TLFR_HD int leaf_node(const Column<float2>& leaves, int k) { return float_as_int_bits(leaves[k].y); }
 
 // Appends leaf node ni (first sample s0) with its key; false when full.
-TLFR_HD bool light_append(const QParams& P, const Query& o, const Column<float2>& leaves, int& nleaves, int ni, int s0)
+TLFR_HD bool leaf_append(const QParams& P, const Query& o, const Column<float2>& leaves, int cap, int& nleaves, int ni,
+                         int s0)
 {
-    if (nleaves == kLLeaf)
+    if (nleaves == cap)
         return false;
     const float4 sp0 = P.s_rec[2 * (s0)];
     const float mvw = P.s_rec[2 * (s0) + 1].z;
@@ -572,17 +573,17 @@ TLFR_HD bool light_append(const QParams& P, const Query& o, const Column<float2>
     return true;
 }
 
-// Light pass, part 1 (RO.cpp:368-407), one output sample per thread: DFS in
-// the reference's order (push child0, child1, pop the last) into the leaf
-// column, then FW::sort of the leaves by key.  Children are stored as pairs,
-// so a node that intersects has both children loaded and tested together and
-// only those that intersect are pushed (a leaf child waits on the stack only
-// behind an internal child1).  The loop has no early exit (an overflow sets a
-// flag), so a warp reconverges at the end of every step.  Returns the leaf
-// count, or -1 when the stack or the leaf column is full.
-TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Column<float2>& leaves, const Query& o)
+// collectInputSamples2's traversal and leaf sort (RO.cpp:368-407) for one output
+// sample at radius R: DFS in the reference's order (push child0, child1, pop the
+// last) into the leaf column, then FW::sort of the leaves by key.  Children are
+// stored as pairs, so a node that intersects has both children loaded and
+// tested together and only those that intersect are pushed (a leaf child waits
+// on the stack only behind an internal child1).  The loop has no early exit (an
+// overflow sets a flag), so a warp reconverges at the end of every step.
+// Returns the leaf count, or -1 when the stack or the leaf column is full.
+TLFR_HD int collect_pairs(const QParams& P, const Column<int>& stack, int stack_cap, const Column<float2>& leaves,
+                          int leaf_cap, const Query& o, float R)
 {
-    const float R = P.disp0;
     int nleaves = 0, sp = 0;
     bool ok = true;
     {
@@ -590,7 +591,7 @@ TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Colu
         if (node_intersect(rn, o, R))
         {
             if (rn.d.x < 0)
-                ok = light_append(P, o, leaves, nleaves, P.root, rn.d.z);
+                ok = leaf_append(P, o, leaves, leaf_cap, nleaves, P.root, rn.d.z);
             else
                 stack[sp++] = rn.d.x;
         }
@@ -601,7 +602,7 @@ TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Colu
     {
         const int e = stack[--sp];
         if (e < 0)
-            ok = light_append(P, o, leaves, nleaves, ~e, P.nodes[~e].d.z);
+            ok = leaf_append(P, o, leaves, leaf_cap, nleaves, ~e, P.nodes[~e].d.z);
         else
         {
             const QNode n0 = P.nodes[e];
@@ -611,7 +612,7 @@ TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Colu
             if (h1 && n1.d.x >= 0)
             {
                 // child1's subtree comes first; child0 waits below it
-                if (sp + 2 > kLStack)
+                if (sp + 2 > stack_cap)
                     ok = false;
                 else
                 {
@@ -623,12 +624,12 @@ TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Colu
             else
             {
                 if (h1)
-                    ok = light_append(P, o, leaves, nleaves, e + 1, n1.d.z);
+                    ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e + 1, n1.d.z);
                 if (h0 && ok)
                 {
                     if (n0.d.x < 0)
-                        ok = light_append(P, o, leaves, nleaves, e, n0.d.z);
-                    else if (sp + 1 > kLStack)
+                        ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e, n0.d.z);
+                    else if (sp + 1 > stack_cap)
                         ok = false;
                     else
                         stack[sp++] = n0.d.x;
@@ -641,6 +642,12 @@ TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Colu
     LLeafSort ls{ leaves };
     fw_sort(ls, 0, nleaves);
     return nleaves;
+}
+
+// Light pass, part 1: each lane collects its own output sample's leaves at 1R.
+TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Column<float2>& leaves, const Query& o)
+{
+    return collect_pairs(P, stack, kLStack, leaves, kLLeaf, o, P.disp0);
 }
 
 // Light pass, part 2 (RO.cpp:94-99, 165-304 for the common case): the 1R scan
