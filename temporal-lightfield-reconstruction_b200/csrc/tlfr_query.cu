@@ -678,51 +678,67 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
     const float RANGE = 1.0f / sqrtf(128.0f);
     const float uvtmin[3] = { o.u - RANGE, o.v - RANGE, o.t - 0.5f * RANGE };
     const float uvtmax[3] = { o.u + RANGE, o.v + RANGE, o.t + 0.5f * RANGE };
-    // sample range of leaf k, held by lane k (the leaf column holds at most 32)
-    int my_s0 = 0, my_s1 = 0;
+    // sample range of leaf k, held by lane k (the leaf column holds at most 32),
+    // and F_k, its offset in the output sample's flat sequence of samples (the
+    // leaves' samples one after another in leaf order)
+    int my_s0 = 0, my_n = 0;
     if (lane < nleaves)
     {
         const int4 d = P.nodes[leaf_node(leaves, lane)].d;
         my_s0 = d.z;
-        my_s1 = d.w;
+        my_n = d.w - d.z;
     }
-    const unsigned nonempty = __ballot_sync(0xffffffffu, my_s0 != my_s1);
-    // chunks of 32 consecutive samples of one leaf, in leaf order; the next
-    // chunk's records are loaded while the current one is processed
-    auto next_leaf = [&](int k) { const unsigned m = nonempty & ~((2u << k) - 1u); return m ? __ffs(m) - 1 : 32; };
-    int lidx = (nonempty & 1u) ? 0 : next_leaf(0);
-    int b = __shfl_sync(0xffffffffu, my_s0, lidx & 31);
-    int s1 = __shfl_sync(0xffffffffu, my_s1, lidx & 31);
-    float4 cpos = make_float4(0, 0, 0, 0), cmot = cpos, ccol = cpos;
-    if (lidx < nleaves && b + lane < s1)
+    int my_f = my_n;
+    for (int off = 1; off < 32; off <<= 1)
     {
-        load_sample(P.s_rec, b + lane, cpos, cmot);
-        ccol = P.s_col[b + lane];
+        const int v = __shfl_up_sync(0xffffffffu, my_f, off);
+        if (lane >= off)
+            my_f += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, my_f, 31);
+    my_f -= my_n;
+    // leaf and sample of flat index f: the last leaf k with F_k <= f (all lanes
+    // call it; lanes with f >= total get an unused answer)
+    auto locate = [&](int f, int& k, int& i) {
+        k = 0;
+        for (int step = 16; step > 0; step >>= 1)
+        {
+            const int c = k + step;
+            const int fc = __shfl_sync(0xffffffffu, my_f, c & 31);
+            if (c < nleaves && fc <= f)
+                k = c;
+        }
+        i = __shfl_sync(0xffffffffu, my_s0, k) + (f - __shfl_sync(0xffffffffu, my_f, k));
+    };
+    // chunks of 32 consecutive flat samples, which may span several leaves; the
+    // next chunk's records are loaded while the current one is processed
+    int ck, ci;
+    locate(lane, ck, ci);
+    bool cvalid = lane < total;
+    float4 cpos = make_float4(0, 0, 0, 0), cmot = cpos, ccol = cpos;
+    if (cvalid)
+    {
+        load_sample(P.s_rec, ci, cpos, cmot);
+        ccol = P.s_col[ci];
     }
     int nsurf = 0, lidx0 = 0, quad = 0, nearest = -1, result = -1, first_leaf = -1;
     float minDist = kF32Max;
     float4 acc = make_float4(0, 0, 0, 0);
-    while (lidx < nleaves && result < 0)
+    for (int base = 0; base < total && result < 0; base += 32)
     {
-        // next chunk and its loads
-        int nlidx = lidx, nb = b + 32, ns1 = s1;
-        if (nb >= s1)
-        {
-            nlidx = next_leaf(lidx);
-            nb = __shfl_sync(0xffffffffu, my_s0, nlidx & 31);
-            ns1 = __shfl_sync(0xffffffffu, my_s1, nlidx & 31);
-        }
+        int nk, ni;
+        locate(base + 32 + lane, nk, ni);
+        const bool nvalid = base + 32 + lane < total;
         float4 npos = make_float4(0, 0, 0, 0), nmot = npos, ncol = npos;
-        if (nlidx < nleaves && nb + lane < ns1)
+        if (nvalid)
         {
-            load_sample(P.s_rec, nb + lane, npos, nmot);
-            ncol = P.s_col[nb + lane];
+            load_sample(P.s_rec, ni, npos, nmot);
+            ncol = P.s_col[ni];
         }
         // the current chunk
-        const int i = b + lane;
         float dx = 0, dy = 0, dist2 = 0;
         bool ok = false;
-        if (i < s1)
+        if (cvalid)
         {
             float x, y;
             if (cmot.x != 0.0f || cmot.y != 0.0f || cmot.z != 0.0f)
@@ -746,51 +762,63 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
             dist2 = dx * dx + dy * dy;
             ok = dist2 <= R2;
         }
-        if (__ballot_sync(0xffffffffu, ok))
+        unsigned accm = __ballot_sync(0xffffffffu, ok);
+        if (accm)
         {
-            if (first_leaf != lidx)
+            const float dist = ok ? sqrtf(dist2) : __int_as_float(0x7f800000);
+            const float weight = 1 - dist / R;
+            const bool inc = ok && weight > 0;
+            const float4 pr = inc ? make_float4(ccol.x * weight, ccol.y * weight, ccol.z * weight, ccol.w * weight)
+                                  : make_float4(0, 0, 0, 0);
+            const int qbit = ok ? 1 << (((dx >= 0 ? 1 : 4) | (dy >= 0 ? 2 : 8)) & 3) : 0;
+            const unsigned incm = __ballot_sync(0xffffffffu, inc);
+            // the chunk's leaves in order, those with accepted samples
+            while (accm)
             {
-                // first accepted sample of this leaf
-                first_leaf = lidx;
-                if (nsurf == 0)
+                const int kseg = __shfl_sync(0xffffffffu, ck, __ffs(accm) - 1);
+                const bool inseg = ck == kseg;
+                const unsigned segm = __ballot_sync(0xffffffffu, inseg);
+                accm &= ~segm;
+                if (first_leaf != kseg)
                 {
-                    nsurf = 1;
-                    lidx0 = lidx;
-                }
-                else
-                {
-                    const QNode cur = P.nodes[leaf_node(leaves, lidx)];
-                    bool same = true;
-                    for (int jb = lidx0; jb < lidx && same; jb += 32)
+                    // first accepted sample of this leaf
+                    first_leaf = kseg;
+                    if (nsurf == 0)
                     {
-                        const int j = jb + lane;
-                        const bool sj = j < lidx ? same_surface(cur, P.nodes[leaf_node(leaves, j)], uvtmin, uvtmax) : true;
-                        same = __all_sync(0xffffffffu, sj);
+                        nsurf = 1;
+                        lidx0 = kseg;
                     }
-                    if (!same)   // a second surface opens: the first one is final
-                        result = (quad == 0xF || first_surface) ? 0 : 1;
+                    else
+                    {
+                        const QNode cur = P.nodes[leaf_node(leaves, kseg)];
+                        bool same = true;
+                        for (int jb = lidx0; jb < kseg && same; jb += 32)
+                        {
+                            const int j = jb + lane;
+                            const bool sj = j < kseg ? same_surface(cur, P.nodes[leaf_node(leaves, j)], uvtmin, uvtmax) : true;
+                            same = __all_sync(0xffffffffu, sj);
+                        }
+                        if (!same)   // a second surface opens: the first one is final
+                        {
+                            result = (quad == 0xF || first_surface) ? 0 : 1;
+                            break;
+                        }
+                    }
                 }
-            }
-            if (result < 0)
-            {
-                quad |= __reduce_or_sync(0xffffffffu, ok ? 1 << (((dx >= 0 ? 1 : 4) | (dy >= 0 ? 2 : 8)) & 3) : 0);
+                const bool sok = ok && inseg;
+                quad |= __reduce_or_sync(0xffffffffu, sok ? qbit : 0);
                 // first strict minimum in sample order (RO.cpp:494-499)
-                const float dist = ok ? sqrtf(dist2) : __int_as_float(0x7f800000);
-                float cmin = dist;
+                float cmin = sok ? dist : __int_as_float(0x7f800000);
                 for (int off = 16; off > 0; off >>= 1)
                     cmin = minr(cmin, __shfl_xor_sync(0xffffffffu, cmin, off));
                 if (cmin < minDist)
                 {
-                    const unsigned at = __ballot_sync(0xffffffffu, ok && dist == cmin);
+                    const unsigned at = __ballot_sync(0xffffffffu, sok && dist == cmin);
                     minDist = cmin;
-                    nearest = __shfl_sync(0xffffffffu, i, __ffs(at) - 1);
+                    nearest = __shfl_sync(0xffffffffu, ci, __ffs(at) - 1);
                 }
-                // tent filter products in parallel, summed in sample order
-                const float weight = 1 - dist / R;
-                const bool inc = ok && weight > 0;
-                const float4 pr = inc ? make_float4(ccol.x * weight, ccol.y * weight, ccol.z * weight, ccol.w * weight)
-                                      : make_float4(0, 0, 0, 0);
-                for (unsigned mi = __ballot_sync(0xffffffffu, inc); mi; mi &= mi - 1)
+                // tent filter products summed in sample order
+                for (unsigned mi = incm & segm; mi; mi &= mi - 1)
                 {
                     const int src = __ffs(mi) - 1;
                     acc.x += __shfl_sync(0xffffffffu, pr.x, src);
@@ -800,7 +828,7 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
                 }
             }
         }
-        lidx = nlidx; b = nb; s1 = ns1;
+        ck = nk; ci = ni; cvalid = nvalid;
         cpos = npos; cmot = nmot; ccol = ncol;
     }
     if (result < 0)
