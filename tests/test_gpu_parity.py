@@ -164,3 +164,31 @@ def test_gpu_full_size_band_matches_oracle():
     for y0 in (0, 537, 1076):
         band = o.reconstruct_rows(y0, y0 + 4)
         assert rel_err(img[y0:y0 + 4], band).max() <= RTOL
+
+
+EDGE = [
+    ("one_row", tlfr.SCENE_CARDS, 17, 1, 4, 41),
+    ("one_column", tlfr.SCENE_CARDS_LARGE, 2, 9, 8, 42),
+    ("tiny_16spp", tlfr.SCENE_PLANES, 3, 2, 16, 43),
+]
+
+
+@pytest.mark.parametrize("name,preset,W,H,spp,seed", EDGE, ids=[e[0] for e in EDGE])
+def test_gpu_degenerate_frames_match_oracle(name, preset, W, H, spp, seed):
+    rec, coc = tlfr.synth_scene(preset, W, H, spp, seed)
+    g = gpu_recon(rec, coc)
+    o = CpuRecon("orc", rec, coc)
+    check_tree(g, o)
+    img = g.reconstructDofMotion()
+    assert np.array_equal(img.view(np.uint32), o.reconstruct().view(np.uint32))
+
+
+def test_gpu_all_samples_discarded_reports_empty():
+    # a 1x1 frame whose only sample reprojects off screen: the reference fails with
+    # "All samples were discarded" (Reconstruction.cpp:587-588); here TLFR_EMPTY
+    rec, coc = tlfr.synth_scene(tlfr.SCENE_CARDS, 1, 1, 1, 5)
+    with pytest.raises(RuntimeError):
+        CpuRecon("orc", rec, coc)
+    with pytest.raises(tlfr.TlfrError) as e:
+        gpu_recon(rec, coc)
+    assert e.value.status == 9   # TLFR_EMPTY

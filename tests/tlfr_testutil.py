@@ -46,6 +46,7 @@ def oracle_lib():
         if not os.path.exists(ORACLE_LIB):
             subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
         _oracle = ctypes.CDLL(ORACLE_LIB)
+        _oracle.orc_last_error.restype = ctypes.c_char_p
     return _oracle
 
 
@@ -78,7 +79,7 @@ class CpuRecon:
                                     ctypes.c_float(aperture), ctypes.c_float(focus), uv, lens, time, output_spp,
                                     nthreads, ctypes.byref(h), ctypes.byref(bs))
             if r:
-                raise RuntimeError(self.lib.orc_last_error and ctypes.string_at(self.lib.orc_last_error()))
+                raise RuntimeError(self.lib.orc_last_error())
         else:
             self.lib = ref_lib(m64)
             os.environ.setdefault("TLFR_REF_THREADS", str(nthreads))
