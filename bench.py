@@ -194,6 +194,17 @@ def train_router(args, device, W, H, S):
     return router, info
 
 
+def max_over_ranks(value, dist, device="cuda"):
+    """The largest value over all ranks (a time measured on every rank); the value itself
+    without a process group."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 BATCH_RES = [(320, 240), (640, 480), (962, 543), (1280, 720), (1920, 1080)]
 BATCH_SPP = [1, 2, 4, 8, 16]
 
@@ -352,10 +363,7 @@ def main():
     barrier()
     clk = clocks.stop()
     total_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist)
     ms_per_step = total_ms / args.steps
     value = (world * Wd * Hd * args.steps / (total_ms / 1e3)) / 1e6
 
@@ -377,10 +385,7 @@ def main():
         r1.record(stream)
         torch.cuda.synchronize()
         r_ms = r0.elapsed_time(r1)
-        if dist:
-            t = torch.tensor([r_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            r_ms = float(t.item())
+        r_ms = max_over_ranks(r_ms, dist)
         rs = tg.stats()
         import numpy as np
         a = out[..., :3].double()
@@ -422,10 +427,7 @@ def main():
         tg.rebuild_from(buf)
         tg.reconstructDofMotion(img)
     e2e_s = (time.perf_counter() - t0) / max(1, args.e2e_steps)
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist)
     e2e = {"value": (world * Wd * Hd / e2e_s) / 1e6, "unit": "Mpix/s", "ms_per_step": e2e_s * 1e3,
            "h2d_bytes_per_step": int(rec.nbytes), "d2h_bytes_per_step": int(img.nbytes)}
 
