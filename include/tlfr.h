@@ -222,7 +222,7 @@ tlfr_status tlfr_synth_scene(int preset, int width, int height, int spp, unsigne
                              float* records, float* coc_out);
 
 /* ---- learned routing (no counterpart in the reference) --------------------
- * The router is the north-star addition: a small network predicts, per pixel,
+ * The router has no counterpart in the reference: a small network predicts, per pixel,
  * whether the fast path reproduces the plain method there; pixels above the
  * threshold take the fast path (the plain 1R pass, which keeps the first
  * surface when a second one opens instead of refetching at 2R; only output

@@ -354,7 +354,7 @@ void free_ctx_buffers(tlfr::Ctx& c)
     void* ptrs[] = { c.own_records ? c.d_records : nullptr, c.rp_pos, c.rp_mot, c.rp_cell, c.hits, c.d_grid,
                      c.cell_count, c.cell_start, c.cell_items, c.kd, c.kd_level, c.kd_leaves_ordered, c.perm, c.box,
                      c.sbounds, c.surface, c.pending, c.leaf_task_rank, c.ordered_n, c.ordered_prefmax, c.top,
-                     c.nodes, c.node_tspan, c.s_rec, c.s_col, c.s_id, c.d_pattern, c.accum, c.qcol, c.heavy_queue, c.ovf_queue,
+                     c.nodes, c.node_tspan, c.s_rec, c.s_col, c.s_id, c.d_pattern, c.qcol, c.heavy_queue, c.ovf_queue,
                      c.ovf_scratch, c.coop_scratch, c.d_stats, c.d_out, c.route_fa, c.route_feats, c.route_prob,
                      c.route_fast, c.route_img };
     for (void* p : ptrs)

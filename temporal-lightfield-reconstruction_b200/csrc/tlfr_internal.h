@@ -163,7 +163,6 @@ struct Ctx
     float4* qcol = nullptr;         // colour of every output sample of the frame
     int*    heavy_queue = nullptr;  // output samples for the full path
     size_t  qcol_cap = 0;
-    float4* accum = nullptr;        // unused
     int*    ovf_queue = nullptr;    // overflowing query ids
     int*    ovf_count = nullptr;
     size_t  ovf_cap = 0;
