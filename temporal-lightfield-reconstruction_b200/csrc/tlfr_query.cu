@@ -81,6 +81,29 @@ TLFR_HD void load_sample(const float4* rec, int i, float4& pos, float4& mot)
 
 enum { kQOk = 0, kQOverflow = 1 };
 
+// Node i (64 bytes, 64-byte aligned) in two 256-bit loads.
+TLFR_HD QNode load_node(const QNode* nodes, int i)
+{
+#ifdef __CUDA_ARCH__
+    unsigned u[16];
+    const QNode* p = nodes + i;
+    asm("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7])
+        : "l"(p));
+    asm("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(u[8]), "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]), "=r"(u[14]), "=r"(u[15])
+        : "l"(reinterpret_cast<const char*>(p) + 32));
+    QNode n;
+    n.a = make_float4(__uint_as_float(u[0]), __uint_as_float(u[1]), __uint_as_float(u[2]), __uint_as_float(u[3]));
+    n.b = make_float4(__uint_as_float(u[4]), __uint_as_float(u[5]), __uint_as_float(u[6]), __uint_as_float(u[7]));
+    n.c = make_float4(__uint_as_float(u[8]), __uint_as_float(u[9]), __uint_as_float(u[10]), __uint_as_float(u[11]));
+    n.d = make_int4((int)u[12], (int)u[13], (int)u[14], (int)u[15]);
+    return n;
+#else
+    return nodes[i];
+#endif
+}
+
 struct LeafSort
 {
     Leaf* l;
@@ -146,7 +169,7 @@ TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& ns
     while (sp > 0)
     {
         const int ni = S.stack[--sp];
-        const QNode node = P.nodes[ni];
+        const QNode node = load_node(P.nodes, ni);
         if (node_intersect(node, o, R))
         {
             if (node.d.x < 0)
@@ -182,7 +205,7 @@ TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& ns
     for (int lidx = 0; lidx < nleaves; lidx++)
     {
         bool first = true;
-        const QNode node = P.nodes[S.leaves[lidx].node];
+        const QNode node = load_node(P.nodes, S.leaves[lidx].node);
         const int s0 = node.d.z, s1 = node.d.w;
         st.in_leaves += (unsigned)(s1 - s0);
         for (int i = s0; i < s1; i++)
@@ -217,7 +240,7 @@ TLFR_HD int collect(const QParams& P, Store& S, const Query& o, float R, int& ns
                     first = false;
                     bool same = true;
                     for (int j = surfaceStart; j < lidx && same; ++j)
-                        same = same_surface(node, P.nodes[S.leaves[j].node], uvtmin, uvtmax);
+                        same = same_surface(node, load_node(P.nodes, S.leaves[j].node), uvtmin, uvtmax);
                     if (!same || nsurf == 0)
                     {
                         surfaceStart = lidx;
@@ -587,7 +610,7 @@ TLFR_HD int collect_pairs(const QParams& P, const Column<int>& stack, int stack_
     int nleaves = 0, sp = 0;
     bool ok = true;
     {
-        const QNode rn = P.nodes[P.root];
+        const QNode rn = load_node(P.nodes, P.root);
         if (node_intersect(rn, o, R))
         {
             if (rn.d.x < 0)
@@ -605,8 +628,8 @@ TLFR_HD int collect_pairs(const QParams& P, const Column<int>& stack, int stack_
             ok = leaf_append(P, o, leaves, leaf_cap, nleaves, ~e, P.nodes[~e].d.z);
         else
         {
-            const QNode n0 = P.nodes[e];
-            const QNode n1 = P.nodes[e + 1];
+            const QNode n0 = load_node(P.nodes, e);
+            const QNode n1 = load_node(P.nodes, e + 1);
             const bool h0 = node_intersect(n0, o, R);
             const bool h1 = node_intersect(n1, o, R);
             if (h1 && n1.d.x >= 0)
@@ -790,12 +813,12 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
                     }
                     else
                     {
-                        const QNode cur = P.nodes[leaf_node(leaves, kseg)];
+                        const QNode cur = load_node(P.nodes, leaf_node(leaves, kseg));
                         bool same = true;
                         for (int jb = lidx0; jb < kseg && same; jb += 32)
                         {
                             const int j = jb + lane;
-                            const bool sj = j < kseg ? same_surface(cur, P.nodes[leaf_node(leaves, j)], uvtmin, uvtmax) : true;
+                            const bool sj = j < kseg ? same_surface(cur, load_node(P.nodes, leaf_node(leaves, j)), uvtmin, uvtmax) : true;
                             same = __all_sync(0xffffffffu, sj);
                         }
                         if (!same)   // a second surface opens: the first one is final
@@ -1036,7 +1059,7 @@ __device__ int traverse_sorted(const QParams& P, const Query& o, float R, Leaf* 
     while (sp > 0)
     {
         const int ni = stack[--sp];
-        const QNode node = P.nodes[ni];
+        const QNode node = load_node(P.nodes, ni);
         if (node_intersect(node, o, R))
         {
             if (node.d.x < 0)
@@ -1081,7 +1104,7 @@ __device__ int coop_scan(const QParams& P, const Query& o, float R, const Leaf* 
     int minIndex = -1, quad = 0, sstart = 0;
     for (int lidx = 0; lidx < nleaves; lidx++)
     {
-        const QNode node = P.nodes[leaves[lidx].node];
+        const QNode node = load_node(P.nodes, leaves[lidx].node);
         const int s0 = node.d.z, s1 = node.d.w;
         bool first = true;
         for (int base = s0; base < s1; base += 32)
@@ -1104,7 +1127,7 @@ __device__ int coop_scan(const QParams& P, const Query& o, float R, const Leaf* 
                 for (int jb = surfaceStart; jb < lidx && same; jb += 32)
                 {
                     const int j = jb + lane;
-                    const bool ok = (j < lidx) ? same_surface(node, P.nodes[leaves[j].node], uvtmin, uvtmax) : true;
+                    const bool ok = (j < lidx) ? same_surface(node, load_node(P.nodes, leaves[j].node), uvtmin, uvtmax) : true;
                     same = __all_sync(0xffffffffu, ok);
                 }
                 if (!same || nsurf == 0)
