@@ -1,7 +1,7 @@
 // tlfr_query.cu — per-output-sample reconstruction on the GPU.
 //
-// One thread answers one output sample (x, y, u, v, t) with the reference's
-// Filterer (reconstruction/ReconstructionOur.cpp:50-511):
+// Every output sample (x, y, u, v, t) is answered with the reference's Filterer
+// (reconstruction/ReconstructionOur.cpp:50-511):
 //   collect(R)   traversal (DFS, child1 popped first), leaf sort by w at the
 //                output time (FW::sort), per-sample reprojection and R test, and
 //                surface separation with sameSurface (Reconstruction.hpp:457-525)
@@ -13,10 +13,19 @@
 // Pixels are the sum of their output samples normalised by alpha, red when
 // nothing was found (Reconstruction.cpp:649-720).
 //
-// Per-query working sets live in thread-local arrays with fixed capacities.  A
-// query that outgrows them is queued and re-run by k_query_overflow with large
-// capacities carved from a global arena; a query that outgrows those too is
-// reported as TLFR_OVERFLOW.
+// The work runs in passes:
+//   k_query_light     every output sample: each lane collects its own leaves at
+//                     1R into shared memory, then the warp scans each lane's
+//                     sample in turn; settles the samples the 1R fetch settles
+//                     (fetch2R false) and queues the rest
+//   k_query_coop      the queue, warp-cooperatively: the full path from the 2R
+//                     fetch (or from 1R for samples that outgrew the light pass)
+//   k_query_overflow  the few samples that outgrow the cooperative pass's lists,
+//                     with large capacities from a global arena; a sample that
+//                     outgrows those too is reported as TLFR_OVERFLOW
+//   k_resolve         pixels from their output samples in sample order
+// plus the statistics, trace and allocation-free variants of the full path, the
+// router's probe pass, and the capture-safe frame pipeline used by batches.
 #include "tlfr_common.cuh"
 #include "tlfr_internal.h"
 
