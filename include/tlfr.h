@@ -274,7 +274,8 @@ tlfr_status tlfr_set_routing(tlfr_ctx* ctx, tlfr_router* router, float threshold
  * Replaces the reference's per-frame reconstruct loop of the animation/export
  * paths (reconstruction_app/App.cpp:616-694).  The graph holds the contexts'
  * buffers as they are at creation: after rebuilding a context with records of
- * another size, create the batch again.  Outputs are device RGBA float images. */
+ * another size, create the batch again.  The contexts (and a router set on one)
+ * must outlive the batch.  Outputs are device RGBA float images. */
 typedef struct tlfr_batch tlfr_batch;
 tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba, void* stream, int autotune,
                               tlfr_batch** out);
