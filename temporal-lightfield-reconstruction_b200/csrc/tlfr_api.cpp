@@ -390,6 +390,9 @@ tlfr_status begin_ctx(const tlfr_params* params, void* stream, int W, int H, int
     cudaError_t e = cudaSetDevice(c.device);
     if (e != cudaSuccess)
         return fail(ctx, TLFR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    e = cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device);
+    if (e != cudaSuccess || c.num_sms <= 0)
+        return fail(ctx, TLFR_CUDA, "cudaDeviceGetAttribute(multiprocessor count): %s", cudaGetErrorString(e));
     c.stream = (cudaStream_t)stream;
     c.W = W; c.H = H; c.spp_in = spp;
     c.n_in = (size_t)W * H * spp;
@@ -1179,7 +1182,7 @@ tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba
     // shared working storage, each frame's buffers, the light pass's grid per
     // frame, one eager run (lazy scratch of the router), then the capture
     {
-        cudaError_t e = cudaMalloc(&b->coop_scratch, tlfr::coop_scratch_bytes());
+        cudaError_t e = cudaMalloc(&b->coop_scratch, tlfr::coop_scratch_bytes(ctxs[0]->c.num_sms));
         if (e == cudaSuccess)
             e = cudaMalloc(&b->ovf_scratch, tlfr::overflow_scratch_bytes());
         if (e != cudaSuccess)
@@ -1206,7 +1209,7 @@ tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba
             float best_ms = 1e30f;
             for (int k : { 2, 4, 8, 16, 32 })
             {
-                const int blocks = std::min(cap, 148 * k);
+                const int blocks = std::min(cap, c.num_sms * k);
                 float ms = 0;
                 st = tlfr::light_trial(c, b->stream, blocks, &ms);
                 if (st != TLFR_OK)

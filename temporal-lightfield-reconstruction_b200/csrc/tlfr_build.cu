@@ -984,10 +984,11 @@ __global__ void k_top(KdNode* kd, GridInfo* g, BNode* pending, BNode* top, QNode
     g->num_nodes = *node_counter;
 }
 
-int grid_for(size_t n, int block)
+int grid_for(const Ctx& c, size_t n, int block)
 {
     size_t b = (n + block - 1) / block;
-    if (b > 148 * 16) b = 148 * 16;
+    const size_t cap = (size_t)c.num_sms * 16;
+    if (b > cap) b = cap;
     return (int)(b ? b : 1);
 }
 
@@ -1023,9 +1024,9 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
     init.bbmax[0] = init.bbmax[1] = 0u;
     CK(cudaMemcpyAsync(acc, &init, sizeof(init), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(counters, 0, 64 * sizeof(int), s));
-    TLFR_LAUNCH(c, k_reproject, grid_for(n, 256), 256, s, rec, n, c.W, c.H, c.coc0_raw[0], c.coc0_raw[1],
+    TLFR_LAUNCH(c, k_reproject, grid_for(c, n, 256), 256, s, rec, n, c.W, c.H, c.coc0_raw[0], c.coc0_raw[1],
                                                  c.rp_pos, c.rp_mot, c.hits, acc);
-    TLFR_LAUNCH(c, k_max_hits, grid_for((size_t)c.W * c.H, 256), 256, s, c.hits, (size_t)c.W * c.H, acc);
+    TLFR_LAUNCH(c, k_max_hits, grid_for(c, (size_t)c.W * c.H, 256), 256, s, c.hits, (size_t)c.W * c.H, acc);
     TLFR_LAUNCH(c, k_grid_setup, 1, 1, s, acc, c.d_grid);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(&c.grid, c.d_grid, sizeof(GridInfo), cudaMemcpyDeviceToHost, s));
@@ -1050,7 +1051,7 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
     if (!c.cell_items)
         CK(cudaMalloc(&c.cell_items, sizeof(int) * n));
     CK(cudaMemsetAsync(c.cell_count, 0, sizeof(int) * (ncell + 1), s));
-    TLFR_LAUNCH(c, k_bucket_count, grid_for(n, 256), 256, s, c.rp_pos, c.rp_mot, n, c.d_grid, c.rp_cell, c.cell_count);
+    TLFR_LAUNCH(c, k_bucket_count, grid_for(c, n, 256), 256, s, c.rp_pos, c.rp_mot, n, c.d_grid, c.rp_cell, c.cell_count);
     {
         const size_t m = ncell + 1;
         const int tiles = (int)((m + kScanTile - 1) / kScanTile);
@@ -1061,8 +1062,8 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
     }
     // scatter with a cursor copy of the starts (reuse cell_count as the cursor)
     CK(cudaMemcpyAsync(c.cell_count, c.cell_start, sizeof(int) * ncell, cudaMemcpyDeviceToDevice, s));
-    TLFR_LAUNCH(c, k_bucket_scatter, grid_for(n, 256), 256, s, c.rp_cell, n, c.cell_count, c.cell_items);
-    TLFR_LAUNCH(c, k_cell_sort, grid_for(ncell, 256), 256, s, c.cell_start, (int)ncell, c.cell_items);
+    TLFR_LAUNCH(c, k_bucket_scatter, grid_for(c, n, 256), 256, s, c.rp_cell, n, c.cell_count, c.cell_items);
+    TLFR_LAUNCH(c, k_cell_sort, grid_for(c, ncell, 256), 256, s, c.cell_start, (int)ncell, c.cell_items);
     CK(cudaGetLastError());
 
     // --- kd split, level by level ---
@@ -1078,13 +1079,13 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
     TLFR_LAUNCH(c, k_kd_init, 1, 1, s, c.kd, c.kd_level, c.d_grid, counters + 0);
     for (int L = 0; L < kMaxKdLevels; L++)
     {
-        TLFR_LAUNCH(c, k_kd_level, 148 * 4, 256, s, c.kd, c.kd_level, L, c.cell_start, c.d_grid, counters + 0);
+        TLFR_LAUNCH(c, k_kd_level, c.num_sms * 4, 256, s, c.kd, c.kd_level, L, c.cell_start, c.d_grid, counters + 0);
         TLFR_LAUNCH(c, k_kd_next, 1, 1, s, c.kd_level, L, counters + 0, c.d_grid);
     }
     for (int L = kMaxKdLevels - 1; L >= 0; L--)
-        TLFR_LAUNCH(c, k_kd_up, 148 * 4, 256, s, c.kd, c.kd_level, L);
+        TLFR_LAUNCH(c, k_kd_up, c.num_sms * 4, 256, s, c.kd, c.kd_level, L);
     for (int L = 0; L < kMaxKdLevels; L++)
-        TLFR_LAUNCH(c, k_kd_down, 148 * 4, 256, s, c.kd, c.kd_level, L);
+        TLFR_LAUNCH(c, k_kd_down, c.num_sms * 4, 256, s, c.kd, c.kd_level, L);
     CK(cudaGetLastError());
     int num_kd = 0;
     CK(cudaMemcpyAsync(&num_kd, counters + 0, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1099,7 +1100,7 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
         }
     }
     TLFR_LAUNCH(c, k_entry_points, 1, 1, s, c.kd, c.d_grid, num_kd);
-    TLFR_LAUNCH(c, k_kd_assign, grid_for(num_kd, 256), 256, s, c.kd, num_kd, c.d_grid, c.kd_leaves_ordered);
+    TLFR_LAUNCH(c, k_kd_assign, grid_for(c, num_kd, 256), 256, s, c.kd, num_kd, c.d_grid, c.kd_leaves_ordered);
     CK(cudaMemcpyAsync(&c.grid, c.d_grid, sizeof(GridInfo), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     const int num_leaves = c.grid.num_kd_leaves;
@@ -1143,21 +1144,21 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
     }
 
     // --- leaves ---
-    TLFR_LAUNCH(c, k_leaf_prepare, grid_for(num_leaves, 128), 128, s, 
+    TLFR_LAUNCH(c, k_leaf_prepare, grid_for(c, num_leaves, 128), 128, s, 
         c.kd_leaves_ordered, num_leaves, c.kd, c.cell_start, c.cell_items, c.d_grid, c.rp_pos, c.rp_mot, rec,
         (float)c.W, (float)c.H, c.coc[0], c.coc[1], c.perm, c.box, c.sbounds, c.s_rec, c.s_col, c.s_id,
         c.ordered_n, counters + 2);
     TLFR_LAUNCH(c, k_task_prefix, 32, 1024, s, c.d_grid, c.ordered_n, c.ordered_prefmax, c.leaf_task_rank);
-    TLFR_LAUNCH(c, k_stale_boxes, grid_for(num_leaves, 128), 128, s, c.kd_leaves_ordered, c.d_grid, c.kd, c.ordered_n,
+    TLFR_LAUNCH(c, k_stale_boxes, grid_for(c, num_leaves, 128), 128, s, c.kd_leaves_ordered, c.d_grid, c.kd, c.ordered_n,
                                                             c.ordered_prefmax, c.leaf_task_rank, c.sbounds, c.box,
                                                             num_leaves, 0);
-    TLFR_LAUNCH(c, k_leaf_scan, grid_for(num_leaves, 128), 128, s, c.kd_leaves_ordered, num_leaves, c.kd, c.s_rec, c.box,
+    TLFR_LAUNCH(c, k_leaf_scan, grid_for(c, num_leaves, 128), 128, s, c.kd_leaves_ordered, num_leaves, c.kd, c.s_rec, c.box,
                                                           c.sbounds, c.surface, c.pending);
     CK(cudaGetLastError());
 
     // --- emitNodes bottom-up, then the serial top ---
     for (int L = c.grid.kd_levels; L >= 5; L--)
-        TLFR_LAUNCH(c, k_emit_level, 148 * 4, 128, s, c.kd, c.kd_level, L, c.pending, c.nodes, c.node_tspan, counters + 1);
+        TLFR_LAUNCH(c, k_emit_level, c.num_sms * 4, 128, s, c.kd, c.kd_level, L, c.pending, c.nodes, c.node_tspan, counters + 1);
     TLFR_LAUNCH(c, k_top, 1, 1, s, c.kd, c.d_grid, c.pending, c.top, c.nodes, c.node_tspan, counters + 1);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(&c.grid, c.d_grid, sizeof(GridInfo), cudaMemcpyDeviceToHost, s));

@@ -98,6 +98,7 @@ struct Ctx
     tlfr_params params{};
     int out_spp = 128;
     int device = 0;
+    int num_sms = 148;              // multiprocessors of the device (read at creation)
     cudaStream_t stream = nullptr;
     std::string error;
 
@@ -201,6 +202,7 @@ struct Route
     __nv_bfloat16* half = nullptr;
     int step = 0;
     int device = 0;
+    int num_sms = 148;          // multiprocessors of the device (read at allocation)
     cudaStream_t stream = nullptr;
     std::string error;
 };
@@ -236,7 +238,7 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats);
 tlfr_status frame_prepare(Ctx& c, bool own_scratch);
 tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_blocks, void* coop_scratch,
                           void* ovf_scratch);
-size_t coop_scratch_bytes();
+size_t coop_scratch_bytes(int num_sms);
 size_t overflow_scratch_bytes();
 tlfr_status frame_hard_failures(Ctx& c, cudaStream_t s, int* hard);
 tlfr_status light_trial(Ctx& c, cudaStream_t s, int light_blocks, float* ms);

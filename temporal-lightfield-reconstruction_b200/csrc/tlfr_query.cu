@@ -701,6 +701,44 @@ TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Colu
 // taken even if its samples do not cover all four quadrants, where the
 // reference would refetch at 2R.  Output samples with nothing within 1R still
 // take the full path.
+// sameSurface's sixteen plane values of one node for one output sample: each
+// bounding plane (xmin, ymin, xmax, ymax) at the lens extremes of the output
+// sample's (u, v) +- RANGE window at the window's middle time, and at the
+// window's two time extremes at the lens centre (Reconstruction.hpp:457-525).
+// Pairs are (low, high) ends in the order the reference tests them.
+struct SurfVals { float v[8][2]; };
+
+TLFR_HD void surf_vals(const QNode& n, const float* uvtmin, const float* uvtmax, SurfVals& s)
+{
+    float a[4][3];
+    node_planes(n, a);
+    const float tmid = 0.5f * (uvtmin[2] + uvtmax[2]);
+    const float ta = uvtmin[2], tb = uvtmax[2];
+    s.v[0][0] = plane_eval(a[0], tmid, uvtmin[0]); s.v[0][1] = plane_eval(a[0], tmid, uvtmax[0]);
+    s.v[1][0] = plane_eval(a[2], tmid, uvtmin[1]); s.v[1][1] = plane_eval(a[2], tmid, uvtmax[1]);
+    s.v[2][0] = plane_eval(a[1], tmid, uvtmin[0]); s.v[2][1] = plane_eval(a[1], tmid, uvtmax[0]);
+    s.v[3][0] = plane_eval(a[3], tmid, uvtmin[1]); s.v[3][1] = plane_eval(a[3], tmid, uvtmax[1]);
+    s.v[4][0] = plane_eval(a[0], ta, 0.0f);        s.v[4][1] = plane_eval(a[0], tb, 0.0f);
+    s.v[5][0] = plane_eval(a[1], ta, 0.0f);        s.v[5][1] = plane_eval(a[1], tb, 0.0f);
+    s.v[6][0] = plane_eval(a[2], ta, 0.0f);        s.v[6][1] = plane_eval(a[2], tb, 0.0f);
+    s.v[7][0] = plane_eval(a[3], ta, 0.0f);        s.v[7][1] = plane_eval(a[3], tb, 0.0f);
+}
+
+// same_surface() from precomputed values: the two nodes differ where, for some
+// plane, one is more than the threshold below the other at one end and more
+// than the threshold above it at the other (ternaryEqual of two opposite
+// ternaryCompare results, Reconstruction.hpp:428-449, 457-525).  The test is
+// symmetric in its arguments.
+TLFR_HD bool same_surface_vals(const SurfVals& a, const SurfVals& b)
+{
+    const float TH = 1 * 0.1f;
+    bool same = true;
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+        same = same && ternary_equal2(ternary_compare(a.v[k][0], b.v[k][0], TH), ternary_compare(a.v[k][1], b.v[k][1], TH));
+    return same;
+}
+
 __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, int nleaves, const Query& o,
                                float4& out, bool first_surface = false)
 {
@@ -712,13 +750,16 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
     const float uvtmax[3] = { o.u + RANGE, o.v + RANGE, o.t + 0.5f * RANGE };
     // sample range of leaf k, held by lane k (the leaf column holds at most 32),
     // and F_k, its offset in the output sample's flat sequence of samples (the
-    // leaves' samples one after another in leaf order)
+    // leaves' samples one after another in leaf order).  Lane k also holds leaf
+    // k's sameSurface values for this output sample.
     int my_s0 = 0, my_n = 0;
+    SurfVals my_sv;
     if (lane < nleaves)
     {
-        const int4 d = P.nodes[leaf_node(leaves, lane)].d;
-        my_s0 = d.z;
-        my_n = d.w - d.z;
+        const QNode nd = load_node(P.nodes, leaf_node(leaves, lane));
+        my_s0 = nd.d.z;
+        my_n = nd.d.w - nd.d.z;
+        surf_vals(nd, uvtmin, uvtmax, my_sv);
     }
     int my_f = my_n;
     for (int off = 1; off < 32; off <<= 1)
@@ -729,23 +770,22 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
     }
     const int total = __shfl_sync(0xffffffffu, my_f, 31);
     my_f -= my_n;
-    // leaf and sample of flat index f: the last leaf k with F_k <= f (all lanes
-    // call it; lanes with f >= total get an unused answer)
-    auto locate = [&](int f, int& k, int& i) {
-        k = 0;
-        for (int step = 16; step > 0; step >>= 1)
-        {
-            const int c = k + step;
-            const int fc = __shfl_sync(0xffffffffu, my_f, c & 31);
-            if (c < nleaves && fc <= f)
-                k = c;
-        }
-        i = __shfl_sync(0xffffffffu, my_s0, k) + (f - __shfl_sync(0xffffffffu, my_f, k));
+    // Leaf and sample of flat index base + lane: the last leaf k with F_k <= f.
+    // Every leaf holds at least one sample (one leaf node per surface run of the
+    // build), so leaf starts are distinct: the leaves starting inside
+    // (base, base + lane] are counted from a mask of the chunk's leaf starts.
+    // All lanes call it; lanes with f >= total get an unused answer.
+    auto locate = [&](int base, int& k, int& i) {
+        const bool starts_in = lane < nleaves && my_f > base && my_f < base + 32;
+        const unsigned starts = __reduce_or_sync(0xffffffffu, starts_in ? 1u << (my_f - base) : 0u);
+        const int kfirst = __popc(__ballot_sync(0xffffffffu, lane < nleaves && my_f <= base)) - 1;
+        k = kfirst + __popc(starts & ((2u << lane) - 1u));
+        i = __shfl_sync(0xffffffffu, my_s0, k & 31) + (base + lane - __shfl_sync(0xffffffffu, my_f, k & 31));
     };
     // chunks of 32 consecutive flat samples, which may span several leaves; the
     // next chunk's records are loaded while the current one is processed
     int ck, ci;
-    locate(lane, ck, ci);
+    locate(0, ck, ci);
     bool cvalid = lane < total;
     float4 cpos = make_float4(0, 0, 0, 0), cmot = cpos, ccol = cpos;
     if (cvalid)
@@ -759,7 +799,7 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
     for (int base = 0; base < total && result < 0; base += 32)
     {
         int nk, ni;
-        locate(base + 32 + lane, nk, ni);
+        locate(base + 32, nk, ni);
         const bool nvalid = base + 32 + lane < total;
         float4 npos = make_float4(0, 0, 0, 0), nmot = npos, ncol = npos;
         if (nvalid)
@@ -822,15 +862,17 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
                     }
                     else
                     {
-                        const QNode cur = load_node(P.nodes, leaf_node(leaves, kseg));
-                        bool same = true;
-                        for (int jb = lidx0; jb < kseg && same; jb += 32)
+                        // lanes j in [lidx0, kseg) test leaf j against this leaf
+                        // (leaf indices are lanes: the column holds at most 32)
+                        SurfVals cur;
+#pragma unroll
+                        for (int a = 0; a < 8; a++)
                         {
-                            const int j = jb + lane;
-                            const bool sj = j < kseg ? same_surface(cur, load_node(P.nodes, leaf_node(leaves, j)), uvtmin, uvtmax) : true;
-                            same = __all_sync(0xffffffffu, sj);
+                            cur.v[a][0] = __shfl_sync(0xffffffffu, my_sv.v[a][0], kseg);
+                            cur.v[a][1] = __shfl_sync(0xffffffffu, my_sv.v[a][1], kseg);
                         }
-                        if (!same)   // a second surface opens: the first one is final
+                        const bool sj = (lane >= lidx0 && lane < kseg) ? same_surface_vals(cur, my_sv) : true;
+                        if (!__all_sync(0xffffffffu, sj))   // a second surface opens: the first one is final
                         {
                             result = (quad == 0xF || first_surface) ? 0 : 1;
                             break;
@@ -839,13 +881,14 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
                 }
                 const bool sok = ok && inseg;
                 quad |= __reduce_or_sync(0xffffffffu, sok ? qbit : 0);
-                // first strict minimum in sample order (RO.cpp:494-499)
-                float cmin = sok ? dist : __int_as_float(0x7f800000);
-                for (int off = 16; off > 0; off >>= 1)
-                    cmin = minr(cmin, __shfl_xor_sync(0xffffffffu, cmin, off));
+                // first strict minimum in sample order (RO.cpp:494-499); distances
+                // are non-negative, so their bit patterns order as unsigned integers
+                const unsigned dbits = sok ? __float_as_uint(dist) : 0x7f800000u;
+                const unsigned mbits = __reduce_min_sync(0xffffffffu, dbits);
+                const float cmin = __uint_as_float(mbits);
                 if (cmin < minDist)
                 {
-                    const unsigned at = __ballot_sync(0xffffffffu, sok && dist == cmin);
+                    const unsigned at = __ballot_sync(0xffffffffu, sok && dbits == mbits);
                     minDist = cmin;
                     nearest = __shfl_sync(0xffffffffu, ci, __ffs(at) - 1);
                 }
@@ -923,9 +966,53 @@ constexpr int kLightBlocksPerSM = 5;
 // PROBE: the router's coarse pass.  Query k of pixel p is output sample
 // (k % kProbe) * M / kProbe (four per pixel); nothing is written but the count of
 // the pixel's probed output samples that the plain 1R pass sends to the full path.
+// Lane -> output sample maps of the light pass.  The 32 lanes of a warp scan
+// each other's leaves one output sample after another, so a warp's output
+// samples should reach nearly the same hierarchy nodes.  The output samples of
+// a pixel are spread over the whole lens and shutter (the reference sorts each
+// pattern's samples by a (u,v,t) Morton key, Reconstruction.cpp:484-510, so
+// sample i of every pattern sits near the same place on that curve):
+//   kMapTiles (M a multiple of 16): an iteration of a block covers a 4x2-pixel
+//     tile and 16 consecutive output samples of each of its pixels; warp w takes
+//     samples 4w..4w+3 of the group, lane l pixel l % 8 and sample l / 8.  The
+//     union of the hierarchy nodes a warp reaches is 3.8x one output sample's
+//     (5.3x for a pixel's 32 consecutive samples) at 1920x1080x8.
+//   kMapLinear: q = block iteration * 128 + thread (the pinhole image's one
+//     sample per pixel, and M not a multiple of 16).
+// Output sample ids q = pixel * M + i are unchanged (qcol, queues).
+enum { kMapLinear = 0, kMapTiles = 1 };
+constexpr int kTileW = 4, kTileH = 2, kTileSamples = 16;
+
+struct LightMap
+{
+    int mode;
+    long long units;        // block iterations
+    int tiles_x;            // kMapTiles: tiles per row
+    int groups;             // kMapTiles: groups of 16 output samples per pixel (M / 16)
+};
+
+// Output sample of thread t in block iteration u; false past the frame's end.
+__device__ __forceinline__ bool light_query_id(const QParams& P, const LightMap& L, long long u, int t,
+                                               long long num_queries, long long& q)
+{
+    if (L.mode == kMapLinear)
+    {
+        q = u * kBlock + t;
+        return q < num_queries;
+    }
+    const long long tile = u / L.groups;
+    const int g = (int)(u - tile * L.groups);
+    const int l = t & 31, p = l & 7;
+    const int x = (int)(tile % L.tiles_x) * kTileW + (p & (kTileW - 1));
+    const int y = (int)(tile / L.tiles_x) * kTileH + p / kTileW;
+    const int i = g * kTileSamples + (t >> 5) * 4 + (l >> 3);
+    q = ((long long)y * P.W + x) * P.M + i;
+    return x < P.W && y < P.H;
+}
+
 template <bool PROBE>
 __global__ void __launch_bounds__(kBlock, kLightBlocksPerSM)
-k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
+k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
               int* __restrict__ heavy_count)
 {
     __shared__ float2 sh_leaves[kLLeaf][kBlock];
@@ -933,11 +1020,11 @@ k_query_light(QParams P, long long num_queries, float4* __restrict__ qcol, int* 
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
     const Column<int> stack{ &sh_stack[0][threadIdx.x], kBlock };
-    for (long long base = (long long)blockIdx.x * kBlock; base < num_queries; base += (long long)gridDim.x * kBlock)
+    for (long long u = blockIdx.x; u < L.units; u += gridDim.x)
     {
         // each lane: traversal and leaf sort of its own output sample
-        const long long q = base + threadIdx.x;
-        const bool valid = q < num_queries;
+        long long q = 0;
+        const bool valid = light_query_id(P, L, u, threadIdx.x, num_queries, q);
         Query o{};
         int nl = -2;
         const long long pix = valid ? (PROBE ? q / kProbe : q / P.M) : 0;
@@ -1023,7 +1110,7 @@ constexpr int kCWarps = 4;
 #ifndef TLFR_COOP_BLOCKS_PER_SM
 #define TLFR_COOP_BLOCKS_PER_SM 8
 #endif
-constexpr int kCoopBlocks = 148 * TLFR_COOP_BLOCKS_PER_SM;
+constexpr int kCoopBlocksPerSM = TLFR_COOP_BLOCKS_PER_SM;
 constexpr int kCLeaf = 256;         // leaves per lane's traversal
 constexpr int kCRs = 4096;          // accepted samples per sample
 constexpr int kCSurf = 512;         // surfaces per sample
@@ -1610,6 +1697,8 @@ QParams make_params(const Ctx& c)
     return P;
 }
 
+int coop_blocks(const Ctx& c) { return c.num_sms * kCoopBlocksPerSM; }
+
 // overflow pass capacities
 constexpr int kOvStack = 512, kOvLeaf = 16384, kOvRs = 65536, kOvSurf = 4096;
 constexpr int kOvSlots = 4096;
@@ -1618,7 +1707,26 @@ constexpr int kOvSlots = 4096;
 
 #define CKQ(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { c.error = std::string(#x) + ": " + cudaGetErrorString(_e); return (_e == cudaErrorMemoryAllocation) ? TLFR_OOM : TLFR_CUDA; } } while (0)
 
-size_t coop_scratch_bytes() { return sizeof(CoopScratch) * (size_t)kCoopBlocks * kCWarps; }
+size_t coop_scratch_bytes(int num_sms) { return sizeof(CoopScratch) * (size_t)num_sms * kCoopBlocksPerSM * kCWarps; }
+
+// light pass iterations and lane map of a frame (nq_probe > 0: the router's
+// probe pass over nq_probe output samples, linear)
+static LightMap light_map(const Ctx& c, long long nq_probe = 0)
+{
+    LightMap L{};
+    if (nq_probe > 0 || c.out_spp % kTileSamples != 0)
+    {
+        const long long nq = nq_probe > 0 ? nq_probe : (long long)c.W * c.H * c.out_spp;
+        L.mode = kMapLinear;
+        L.units = (nq + kBlock - 1) / kBlock;
+        return L;
+    }
+    L.mode = kMapTiles;
+    L.tiles_x = (c.W + kTileW - 1) / kTileW;
+    L.groups = c.out_spp / kTileSamples;
+    L.units = (long long)L.tiles_x * ((c.H + kTileH - 1) / kTileH) * L.groups;
+    return L;
+}
 size_t overflow_scratch_bytes() { return slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf) * kOvSlots; }
 
 tlfr_status route_probe(Ctx& c, int* d_counts)
@@ -1633,8 +1741,9 @@ tlfr_status route_probe(Ctx& c, int* d_counts)
     }
     QParams P = make_params(c);
     CKQ(cudaMemsetAsync(d_counts, 0, sizeof(int) * npix, s));
-    const int blocks = (int)std::min<long long>((nq + kBlock - 1) / kBlock, 148LL * 64);
-    TLFR_LAUNCH(c, k_query_light<true>, blocks, kBlock, s, P, nq, nullptr, nullptr, d_counts);
+    const LightMap L = light_map(c, nq);
+    const int blocks = (int)std::min<long long>(L.units, (long long)c.num_sms * 64);
+    TLFR_LAUNCH(c, k_query_light<true>, blocks, kBlock, s, P, L, nq, nullptr, nullptr, d_counts);
     CKQ(cudaGetLastError());
     return TLFR_OK;
 }
@@ -1664,7 +1773,7 @@ tlfr_status frame_prepare(Ctx& c, bool own_scratch)
         CKQ(cudaMalloc(&c.d_stats, sizeof(DevStats) + 8 * sizeof(int)));
     if (own_scratch && !c.coop_scratch)
     {
-        c.coop_scratch_bytes = coop_scratch_bytes();
+        c.coop_scratch_bytes = coop_scratch_bytes(c.num_sms);
         CKQ(cudaMalloc(&c.coop_scratch, c.coop_scratch_bytes));
     }
     if (own_scratch && !c.ovf_scratch)
@@ -1683,8 +1792,8 @@ tlfr_status frame_prepare(Ctx& c, bool own_scratch)
 
 int light_default_blocks(const Ctx& c)
 {
-    const long long nq = (long long)c.W * c.H * c.out_spp;
-    return (int)std::min<long long>((nq + kBlock - 1) / kBlock, 148LL * 64);
+    const LightMap L = light_map(c);
+    return (int)std::min<long long>(L.units, (long long)c.num_sms * 64);
 }
 
 // One frame's reconstruction issued on stream s with no host synchronisation:
@@ -1724,14 +1833,15 @@ tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_bloc
         c.launches++;
         P.route_fast = c.route_fast;
     }
-    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, nq, c.qcol, c.heavy_queue, counters + 2);
-    TLFR_LAUNCH(c, k_query_coop, kCoopBlocks, kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol, c.ovf_queue,
+    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
+                counters + 2);
+    TLFR_LAUNCH(c, k_query_coop, coop_blocks(c), kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol, c.ovf_queue,
                 counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(coop_scratch));
     TLFR_LAUNCH(c, k_query_overflow, kOvSlots / 64, 64, s, P, c.ovf_queue, counters + 0, (int)c.ovf_cap, c.qcol,
                 (char*)ovf_scratch, slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf), kOvSlots, kOvStack, kOvLeaf,
                 kOvRs, kOvSurf, counters + 1, c.d_stats, 0);
-    TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, 148LL * 32), 128, s, c.qcol, c.out_spp,
-                d_rgba, npix);
+    TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, (long long)c.num_sms * 32), 128, s, c.qcol,
+                c.out_spp, d_rgba, npix);
     c.stream = saved;
     CKQ(cudaGetLastError());
     return TLFR_OK;
@@ -1757,7 +1867,8 @@ tlfr_status light_trial(Ctx& c, cudaStream_t s, int light_blocks, float* ms)
     CKQ(cudaEventCreate(&e1));
     CKQ(cudaMemsetAsync(counters, 0, 8 * sizeof(int), s));
     CKQ(cudaEventRecord(e0, s));
-    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, nq, c.qcol, c.heavy_queue, counters + 2);
+    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
+                counters + 2);
     CKQ(cudaEventRecord(e1, s));
     CKQ(cudaEventSynchronize(e1));
     CKQ(cudaEventElapsedTime(ms, e0, e1));
@@ -1806,7 +1917,7 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
         CKQ(cudaMemsetAsync(c.route_fast, 1, npix, s));
         P.route_fast = c.route_fast;
     }
-    const int blocks = (int)std::min<long long>((nq + kBlock - 1) / kBlock, 148LL * 64);
+    const int blocks = (int)std::min<long long>((nq + kBlock - 1) / kBlock, (long long)c.num_sms * 64);
     if (!c.evq0)
     {
         CKQ(cudaEventCreate(&c.evq0));
@@ -1839,15 +1950,15 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
     }
     else
     {
-        const int coop_blocks = kCoopBlocks;
         if (!c.coop_scratch)
         {
-            c.coop_scratch_bytes = coop_scratch_bytes();
+            c.coop_scratch_bytes = coop_scratch_bytes(c.num_sms);
             CKQ(cudaMalloc(&c.coop_scratch, c.coop_scratch_bytes));
         }
-        TLFR_LAUNCH(c, k_query_light<false>, blocks, kBlock, s, P, nq, c.qcol, c.heavy_queue, counters + 2);
+        TLFR_LAUNCH(c, k_query_light<false>, light_default_blocks(c), kBlock, s, P, light_map(c), nq, c.qcol,
+                    c.heavy_queue, counters + 2);
         CKQ(cudaEventRecord(c.evq1, s));
-        TLFR_LAUNCH(c, k_query_coop, coop_blocks, kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol,
+        TLFR_LAUNCH(c, k_query_coop, coop_blocks(c), kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol,
                     c.ovf_queue, counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(c.coop_scratch));
     }
     CKQ(cudaEventRecord(c.evq2, s));
@@ -1878,8 +1989,8 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
         CKQ(cudaGetLastError());
         CKQ(cudaMemcpyAsync(&hard, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     }
-    TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, 148LL * 32), 128, s, c.qcol, c.out_spp,
-                d_rgba, npix);
+    TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, (long long)c.num_sms * 32), 128, s, c.qcol,
+                c.out_spp, d_rgba, npix);
     CKQ(cudaGetLastError());
     {
         float ms = 0, ms2 = 0;

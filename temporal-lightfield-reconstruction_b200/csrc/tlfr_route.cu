@@ -563,6 +563,7 @@ int route_num_trainable() { return kNumTrain; }
 
 tlfr_status route_alloc(Route& r, std::string& err)
 {
+    CKR(cudaDeviceGetAttribute(&r.num_sms, cudaDevAttrMultiProcessorCount, r.device));
     CKR(cudaMalloc(&r.params, sizeof(float) * kNumParams));
     CKR(cudaMalloc(&r.grad, sizeof(float) * kNumTrain));
     CKR(cudaMalloc(&r.m, sizeof(float) * kNumTrain));
@@ -632,14 +633,17 @@ tlfr_status route_get_params(Route& r, float* host_params, cudaStream_t s, std::
     return TLFR_OK;
 }
 
-static int train_blocks(int batch) { return std::max(1, std::min(148 * 4, (batch + 16 * kTrainWarps - 1) / (16 * kTrainWarps))); }
+static int train_blocks(const Route& r, int batch)
+{
+    return std::max(1, std::min(r.num_sms * 4, (batch + 16 * kTrainWarps - 1) / (16 * kTrainWarps)));
+}
 
 tlfr_status route_gradient(Route& r, const float* d_feats, const float* d_labels, int n, float* host_grad,
                            float* host_loss, cudaStream_t s, std::string& err)
 {
     CKR(cudaMemsetAsync(r.grad, 0, sizeof(float) * kNumTrain, s));
     CKR(cudaMemsetAsync(r.loss, 0, sizeof(float), s));
-    k_mlp_train<<<train_blocks(n), kTrainWarps * 32, 0, s>>>(r.params, r.half, d_feats, d_labels, n, n, 0, 0, 1,
+    k_mlp_train<<<train_blocks(r, n), kTrainWarps * 32, 0, s>>>(r.params, r.half, d_feats, d_labels, n, n, 0, 0, 1,
                                                              r.grad, r.loss);
     CKR(cudaGetLastError());
     CKR(cudaMemcpyAsync(host_grad, r.grad, sizeof(float) * kNumTrain, cudaMemcpyDeviceToHost, s));
@@ -661,7 +665,7 @@ tlfr_status route_train(Route& r, const float* d_feats, const float* d_labels, i
         const bool last = k == steps - 1;
         if (last)
             CKR(cudaMemsetAsync(r.loss, 0, sizeof(float), s));
-        k_mlp_train<<<train_blocks(batch), kTrainWarps * 32, 0, s>>>(r.params, r.half, d_feats, d_labels, n, batch,
+        k_mlp_train<<<train_blocks(r, batch), kTrainWarps * 32, 0, s>>>(r.params, r.half, d_feats, d_labels, n, batch,
                                                                      seed, (unsigned)r.step, 0, r.grad, r.loss);
         k_adam<<<(kNumTrain + 255) / 256, 256, 0, s>>>(r.params, r.grad, r.m, r.v, lr, b1, b2, eps,
                                                        1.0f - powf(b1, (float)r.step), 1.0f - powf(b2, (float)r.step));
@@ -677,7 +681,7 @@ tlfr_status route_train(Route& r, const float* d_feats, const float* d_labels, i
 tlfr_status route_predict(Route& r, const float* d_feats, long long n, float* d_prob, cudaStream_t s, std::string& err)
 {
     const long long tiles = (n + 15) / 16;
-    const int blocks = (int)std::max(1LL, std::min(148LL * 8, (tiles + 3) / 4));
+    const int blocks = (int)std::max(1LL, std::min((long long)r.num_sms * 8, (tiles + 3) / 4));
     k_mlp_infer<<<blocks, 128, 0, s>>>(r.params, r.half, d_feats, n, d_prob);
     CKR(cudaGetLastError());
     return TLFR_OK;
@@ -695,7 +699,7 @@ tlfr_status route_features(Ctx& c, float* d_feats, std::string& err)
     float4* fb = c.route_fa + npix;
     float4* tiles = c.route_fa + 2 * npix;
     int* probe = reinterpret_cast<int*>(c.route_fa + 2 * npix + (size_t)TW * TH);
-    const int blocks = (int)std::max(1LL, std::min(148LL * 16, (npix + 255) / 256));
+    const int blocks = (int)std::max(1LL, std::min((long long)c.num_sms * 16, (npix + 255) / 256));
     k_feat_pixel<<<blocks, 256, 0, c.stream>>>(c.cur_records, c.hits, npix, c.spp_in, c.coc[0], c.coc[1], fa, fb);
     k_feat_tile<<<(TW * TH + 127) / 128, 128, 0, c.stream>>>(fa, c.W, c.H, TW, TH, tiles);
     const tlfr_status ps = route_probe(c, probe);
@@ -714,7 +718,7 @@ tlfr_status route_labels_from(Ctx& c, const float4* d_plain, const float4* d_fas
                               std::string& err)
 {
     const long long npix = (long long)c.W * c.H;
-    const int blocks = (int)std::max(1LL, std::min(148LL * 16, (npix + 255) / 256));
+    const int blocks = (int)std::max(1LL, std::min((long long)c.num_sms * 16, (npix + 255) / 256));
     k_labels<<<blocks, 256, 0, c.stream>>>(d_plain, d_fast, npix, tol, d_labels);
     c.launches++;
     CKR(cudaGetLastError());
@@ -724,7 +728,7 @@ tlfr_status route_labels_from(Ctx& c, const float4* d_plain, const float4* d_fas
 tlfr_status route_flags(Ctx& c, const float* d_prob, float hi, unsigned char* d_fast, std::string& err)
 {
     const long long npix = (long long)c.W * c.H;
-    const int blocks = (int)std::max(1LL, std::min(148LL * 16, (npix + 255) / 256));
+    const int blocks = (int)std::max(1LL, std::min((long long)c.num_sms * 16, (npix + 255) / 256));
     k_route_flags<<<blocks, 256, 0, c.stream>>>(d_prob, npix, hi, d_fast);
     c.launches++;
     CKR(cudaGetLastError());
