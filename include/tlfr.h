@@ -194,16 +194,20 @@ tlfr_status tlfr_trace_queries(tlfr_ctx* ctx, const int* xyi, int num_queries,
  * memory reserved up front, an external allocator that owns the device heap, a
  * thread that must not block on the allocator).  Same results as the colours of
  * tlfr_trace_queries, for the output samples (x, y, i) in d_xyi[3*k ..] (device
- * memory), written to d_rgba[4*k ..] (device memory).  The per-query working
- * storage is a fixed 10.25 MiB device array inside the library (256 working
- * slots), which every device that loads the library keeps until the process
- * exits; nothing is allocated by the call.  A query that needs more than a slot
- * holds (or an (x, y, i) out of range) yields (0, 0, 0, -1) and is counted in
- * *d_overflow (device memory, may be NULL; set to zero by the call).
- * num_queries <= 4194304 per call, else TLFR_BAD_ARG.  Asynchronous on the
- * context's stream.  The first call on a device looks up the array's device
- * address with that device current: make it before any stream capture.  All
- * calls share the array, so calls whose work overlaps on the GPU race.       */
+ * memory, 4-byte aligned), written to d_rgba[4*k ..] (device memory, 16-byte
+ * aligned: the colours are stored as float4; a misaligned pointer is refused
+ * with TLFR_BAD_ARG).  The per-query working storage is a fixed 9.75 MiB device
+ * array inside the library (256 working slots), which every device that loads
+ * the library keeps until the process exits; nothing is allocated by the call.
+ * A query that needs more than a slot holds (or an (x, y, i) out of range)
+ * yields (0, 0, 0, -1) and is counted in *d_overflow (device memory, may be
+ * NULL; set to zero by the call, also when num_queries is 0).
+ * num_queries <= 262144 per call, else TLFR_BAD_ARG: the 256 slots each run one
+ * query at a time, so a call is meant for a few thousand to a few hundred
+ * thousand output samples.  Asynchronous on the context's stream.  The first
+ * call on a device looks up the array's device address with that device
+ * current: make it before any stream capture.  All calls share the array, so
+ * calls whose work overlaps on the GPU race.                                   */
 tlfr_status tlfr_query_samples_noalloc(tlfr_ctx* ctx, const int* d_xyi, int num_queries, float* d_rgba,
                                        int* d_overflow);
 

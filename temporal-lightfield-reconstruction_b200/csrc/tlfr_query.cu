@@ -2083,11 +2083,11 @@ tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h
 // allocator, code that owns the device heap through its own allocator) can still
 // reconstruct individual output samples.  The per-query working storage that
 // tlfr_trace_queries allocates per call lives here in one fixed device array
-// instead: kNaSlots working slots of kNaSlotBytes each (kNaSlots * kNaSlotBytes
-// = 10.25 MiB), which every device that loads this library keeps until the
-// process exits.  Each slot runs the full per-sample path with capacities
-// kNaStack / kNaLeaf / kNaRs / kNaSurf; a query that needs more is reported as
-// (0, 0, 0, -1) and counted, not retried.
+// instead: kNaSlots working slots of kNaSlotBytes each (9.75 MiB in all), which
+// every device that loads this library keeps until the process exits.  Each
+// slot runs the full per-sample path with capacities kNaStack / kNaLeaf /
+// kNaRs / kNaSurf; a query that needs more is reported as (0, 0, 0, -1) and
+// counted, not retried.
 //
 // All calls share the array: two calls whose kernels overlap on the GPU (on
 // different streams, or from different contexts on the same device) race on it.
@@ -2100,16 +2100,18 @@ constexpr int kNaStack = 96, kNaLeaf = 512, kNaRs = 2048, kNaSurf = 128;
 constexpr size_t kNaSlotBytes =
     (sizeof(int) * kNaStack + sizeof(Leaf) * kNaLeaf + sizeof(RSample) * kNaRs + sizeof(Surf) * kNaSurf + 255) &
     ~(size_t)255;
-constexpr int kNaMaxQueries = 1 << 22;
+constexpr size_t kNaArenaBytes = kNaSlots * kNaSlotBytes;
+static_assert(kNaArenaBytes == 10223616, "the documented size of the fixed array (9.75 MiB) follows the constants");
+constexpr int kNaMaxQueries = 1 << 18;
 constexpr int kNaMaxDevices = 64;
 }
 
-static __device__ __align__(256) unsigned char g_noalloc_arena[kNaSlots * kNaSlotBytes];
+static __device__ __align__(256) unsigned char g_noalloc_arena[kNaArenaBytes];
 
 namespace
 {
 
-__global__ void __launch_bounds__(64)
+__global__ void __launch_bounds__(32)
 k_query_noalloc(QParams P, const int* __restrict__ xyi, int n, float4* __restrict__ rgba, unsigned char* arena,
                 int* overflow)
 {
@@ -2143,7 +2145,10 @@ k_query_noalloc(QParams P, const int* __restrict__ xyi, int n, float4* __restric
 }
 
 // Device address of g_noalloc_arena for each device, looked up on the first
-// call made with that device current.
+// call made with that device current.  A later call checks that the address
+// still belongs to the device (cudaPointerGetAttributes allocates nothing) and
+// looks it up again when it does not (after a cudaDeviceReset the module and
+// its array are loaded anew).
 std::mutex g_na_lock;
 void* g_na_ptr[kNaMaxDevices] = {};
 
@@ -2157,6 +2162,19 @@ tlfr_status query_samples_noalloc(Ctx& c, const int* d_xyi, int n, float* d_rgba
                   std::to_string(kNaMaxQueries) + "]";
         return TLFR_BAD_ARG;
     }
+    // colours are written as float4 and queries read as int: a misaligned
+    // pointer would fault the kernel
+    if (n > 0 && (!d_xyi || !d_rgba || (reinterpret_cast<uintptr_t>(d_rgba) & 15) != 0 ||
+                  (reinterpret_cast<uintptr_t>(d_xyi) & 3) != 0))
+    {
+        c.error = "tlfr_query_samples_noalloc: d_rgba must be 16-byte aligned and d_xyi 4-byte aligned (non-null)";
+        return TLFR_BAD_ARG;
+    }
+    if (d_overflow && (reinterpret_cast<uintptr_t>(d_overflow) & 3) != 0)
+    {
+        c.error = "tlfr_query_samples_noalloc: d_overflow must be 4-byte aligned";
+        return TLFR_BAD_ARG;
+    }
     if (c.device < 0 || c.device >= kNaMaxDevices)
     {
         c.error = "tlfr_query_samples_noalloc: device ordinal beyond the supported " + std::to_string(kNaMaxDevices);
@@ -2165,18 +2183,29 @@ tlfr_status query_samples_noalloc(Ctx& c, const int* d_xyi, int n, float* d_rgba
     void* arena = nullptr;
     {
         std::lock_guard<std::mutex> g(g_na_lock);
-        if (!g_na_ptr[c.device])
+        void*& cached = g_na_ptr[c.device];
+        if (cached)
+        {
+            cudaPointerAttributes a{};
+            if (cudaPointerGetAttributes(&a, cached) != cudaSuccess || a.type != cudaMemoryTypeDevice ||
+                a.device != c.device)
+            {
+                cudaGetLastError();
+                cached = nullptr;
+            }
+        }
+        if (!cached)
         {
             // the context's device is current (set by the caller of this function)
-            cudaError_t e = cudaGetSymbolAddress(&g_na_ptr[c.device], g_noalloc_arena);
+            cudaError_t e = cudaGetSymbolAddress(&cached, g_noalloc_arena);
             if (e != cudaSuccess)
             {
-                g_na_ptr[c.device] = nullptr;
+                cached = nullptr;
                 c.error = std::string("tlfr_query_samples_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
                 return TLFR_CUDA;
             }
         }
-        arena = g_na_ptr[c.device];
+        arena = cached;
     }
     if (d_overflow)
     {
@@ -2190,7 +2219,8 @@ tlfr_status query_samples_noalloc(Ctx& c, const int* d_xyi, int n, float* d_rgba
     if (n == 0)
         return TLFR_OK;
     QParams P = make_params(c);
-    TLFR_LAUNCH(c, k_query_noalloc, kNaSlots / 64, 64, c.stream, P, d_xyi, n, reinterpret_cast<float4*>(d_rgba),
+    // 32-thread blocks spread the slots over kNaSlots / 32 multiprocessors
+    TLFR_LAUNCH(c, k_query_noalloc, kNaSlots / 32, 32, c.stream, P, d_xyi, n, reinterpret_cast<float4*>(d_rgba),
                 static_cast<unsigned char*>(arena), d_overflow);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
