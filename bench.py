@@ -48,6 +48,7 @@ METRIC = "recon Mpix/s on 1 B200: learned-routed vs plain GPU at <=0.1 dB loss; 
 W, H, SPP, M = 1920, 1080, 8, 128
 PRESET = 2
 WORKLOAD = "1920x1080 8spp defocus+motion, 256 rects + 64 disks, 128 output samples/px"
+DATA = "synthetic (seeded analytic scene)"
 
 
 def parse():
@@ -58,7 +59,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-rows", type=int, default=8, help="rows per CPU baseline sample")
+    ap.add_argument("--cpu-rows", type=int, default=8, help="rows per CPU sample (spread over the frame)")
     ap.add_argument("--width", type=int, default=W)
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
@@ -145,24 +146,86 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline_sample(rec, coc, rows, threads):
-    """Reference CPU reconstruction timed on this host: full build + `rows` rows."""
-    from tlfr_testutil import CpuRecon, ref_available
-    kind = "reference" if ref_available() else "port"
-    os.environ["TLFR_REF_THREADS"] = str(threads)
-    r = CpuRecon("ref" if kind == "reference" else "orc", rec, coc, nthreads=threads)
-    Hh, Ww = rec.shape[0], rec.shape[1]
-    y0 = Hh // 2 - rows // 2
-    r.reconstruct_rows(y0, y0 + rows)
-    band = r.last_seconds
-    est = r.build_seconds + band * (Hh / rows)
-    r.close()
-    return {
-        "value": (Ww * Hh / est) / 1e6, "unit": "Mpix/s", "cores": threads, "kind": kind,
-        "sample": f"full {Ww}x{Hh} hierarchy build ({r.build_seconds:.2f} s) + rows [{y0},{y0 + rows}) of the query "
-                  f"({band:.2f} s), extrapolated to {Hh} rows",
-        "build_s": r.build_seconds, "band_s": band,
+def cpu_rows(height, rows, step):
+    """`rows` rows spread evenly over the frame, the comb shifted per step (golden
+    ratio), so that successive samples cover different rows."""
+    stride = height / rows
+    off = (0.5 + 0.6180339887 * step) % 1.0
+    return sorted({min(height - 1, int((j + off) * stride)) for j in range(rows)})
+
+
+def ref_scene(width, height, spp, seed):
+    """The seeded scene from the reference build's own copy of the generator
+    (oracle/_ref), so that the reference's CPU runs load no library of this
+    package; the package's generator when the reference build is absent."""
+    import ctypes
+    import numpy as np
+    from tlfr_testutil import ref_available, ref_lib
+    if not ref_available():
+        import tlfr
+        return tlfr.synth_scene(PRESET, width, height, spp, seed)
+    lib = ref_lib()
+    rec = np.empty((height, width, spp, 16), np.float32)
+    coc = np.zeros(2, np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    st = lib.ref_synth_scene(PRESET, width, height, spp, ctypes.c_ulonglong(seed), rec.ctypes.data_as(fp),
+                             coc.ctypes.data_as(fp))
+    if st != 0:
+        raise RuntimeError(f"ref_synth_scene failed ({st})")
+    return rec, (float(coc[0]), float(coc[1]))
+
+
+class CpuSampler:
+    """The reference's own CPU reconstruction (oracle/_ref; the C restatement
+    when the reference build is absent) of one frame on this host's cores: the
+    full hierarchy build once, then per sample a comb of rows spread over the
+    frame.  The frame time is estimated as build + (query time of the rows) x
+    height / rows.  Both the reference arm and the GPU arm's cpu_baseline use it."""
+
+    def __init__(self, rec, coc, threads):
+        from tlfr_testutil import CpuRecon, ref_available
+        self.kind = "reference" if ref_available() else "port"
+        os.environ["TLFR_REF_THREADS"] = str(threads)
+        self.threads = threads
+        self.r = CpuRecon("ref" if self.kind == "reference" else "orc", rec, coc, nthreads=threads)
+        self.H, self.W = rec.shape[0], rec.shape[1]
+        self.build_s = self.r.build_seconds
+
+    def sample(self, rows, step):
+        ys = cpu_rows(self.H, rows, step)
+        t, imgs = 0.0, {}
+        for y in ys:
+            imgs[y] = self.r.reconstruct_rows(y, y + 1)[0]
+            t += self.r.last_seconds
+        est = self.build_s + t * self.H / len(ys)
+        return est, t, ys, imgs
+
+    def close(self):
+        self.r.close()
+
+
+def cpu_baseline_sample(rec, coc, rows, threads, gpu_img=None):
+    """cpu_baseline of the GPU arm, plus a parity check of the timed GPU frame:
+    the sampled rows of the reference's CPU image against the same rows of the
+    GPU image (outside every timed region)."""
+    import numpy as np
+    cs = CpuSampler(rec, coc, threads)
+    est, t, ys, imgs = cs.sample(rows, 0)
+    cs.close()
+    out = {
+        "value": (cs.W * cs.H / est) / 1e6, "unit": "Mpix/s", "cores": threads, "kind": cs.kind,
+        "sample": f"full {cs.W}x{cs.H} hierarchy build ({cs.build_s:.2f} s) + {len(ys)} rows spread over the frame "
+                  f"({t:.2f} s), extrapolated to {cs.H} rows",
+        "build_s": cs.build_s, "rows_s": t, "rows": ys,
     }
+    if gpu_img is not None:
+        cpu = np.stack([imgs[y] for y in ys])
+        gpu = np.stack([gpu_img[y] for y in ys])
+        rel = np.abs(gpu - cpu) / np.maximum(np.abs(cpu), 1e-6)
+        out["parity"] = {"rows": ys, "pixels": int(cpu.shape[0] * cpu.shape[1]),
+                         "bit_exact": bool(np.array_equal(gpu.view(np.uint32), cpu.view(np.uint32))),
+                         "max_rel_err": float(rel.max()), "tolerance": 1e-4, "ok": bool(rel.max() <= 1e-4)}
+    return out
 
 
 def train_router(args, device, W, H, S):
@@ -266,67 +329,36 @@ def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation on the host cores."""
     if rank != 0:
         return
-    import tlfr
-    from tlfr_testutil import CpuRecon, ref_available
     threads = os.cpu_count() or 1
-    kind = "reference" if ref_available() else "port"
-    os.environ["TLFR_REF_THREADS"] = str(threads)
-    rec, coc = tlfr.synth_scene(PRESET, args.width, args.height, args.spp, 2)
-    r = CpuRecon("ref" if kind == "reference" else "orc", rec, coc, nthreads=threads)
-    rows = max(1, args.cpu_rows // 2)
-    vals = []
-    Hh = args.height
+    rec, coc = ref_scene(args.width, args.height, args.spp, 2)
+    cs = CpuSampler(rec, coc, threads)
+    rows = max(1, args.cpu_rows)
+    ests, ts = [], []
     for k in range(args.warmup + args.steps):
-        y0 = (Hh // 2 + 37 * k) % (Hh - rows)
-        r.reconstruct_rows(y0, y0 + rows)
-        est = r.build_seconds + r.last_seconds * (Hh / rows)
+        est, t, ys, _ = cs.sample(rows, k)
         if k >= args.warmup:
-            vals.append(est)
-    t = statistics.median(vals)
-    value = (args.width * Hh / t) / 1e6
-    sample = (f"full {args.width}x{Hh} hierarchy build ({r.build_seconds:.2f} s, once) + per step {rows} rows of the "
-              f"query, extrapolated to the frame")
+            ests.append(est)
+            ts.append(t)
+    cs.close()
+    est = statistics.median(ests)
+    value = (args.width * args.height / est) / 1e6
+    sample = (f"full {args.width}x{args.height} hierarchy build ({cs.build_s:.2f} s, once) + per step {rows} rows "
+              f"spread over the frame (comb shifted per step); frame time = build + rows' time x "
+              f"{args.height}/{rows}; ms_per_step = the rows' measured time")
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic scene)", "impl": "reference",
-        "config": {"workload": WORKLOAD, "width": args.width, "height": Hh, "spp": args.spp, "output_spp": M},
-        "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": threads, "kind": kind, "sample": sample},
+        "warmup": args.warmup, "ms_per_step": statistics.mean(ts) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA, "impl": "reference",
+        "config": bench_config(args), "frame_s_estimate": est,
+        "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": threads, "kind": cs.kind, "sample": sample},
         "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def run_profile_frame(args):
-    """One frame reconstructed from device-resident records: hierarchy build and
-    query passes timed with CUDA events per step (no CPU baseline, no router,
-    no batch).  Used for profiler captures of single kernels."""
-    import torch
-    import tlfr
-    torch.cuda.set_device(0)
-    Wd, Hd, S = args.width, args.height, args.spp
-    rec, coc = tlfr.synth_scene(args.scene, Wd, Hd, S, 2)
-    d_rec = torch.from_numpy(rec).cuda()
-    stream = torch.cuda.current_stream()
-    tg = tlfr.TreeGather(None, tlfr.CameraParams(device=0), stream=stream.cuda_stream,
-                         device_records=(d_rec.data_ptr(), (Wd, Hd, S), coc))
-    out = torch.empty((Hd, Wd, 4), dtype=torch.float32, device="cuda")
-    rows = []
-    for k in range(args.warmup + args.steps):
-        tg.rebuild(d_rec.data_ptr())
-        b = tg.stats().build_ms
-        tg.reconstruct_to_device(out.data_ptr())
-        st = tg.stats()
-        if k >= args.warmup:
-            rows.append((b, st.light_ms, st.heavy_ms, st.query_kernel_ms, st.num_heavy_queries))
-    torch.cuda.synchronize()
-    med = lambda i: statistics.median(r[i] for r in rows)
-    line = {"profile_frame": f"{Wd}x{Hd}x{S}", "scene": args.scene, "steps": args.steps, "warmup": args.warmup,
-            "build_ms": med(0), "light_ms": med(1), "heavy_ms": med(2), "query_kernel_ms": med(3),
-            "heavy_queries": int(rows[-1][4]), "output_samples": Wd * Hd * M,
-            "checksum": float(out.double().sum().item())}
-    tg.close()
-    print(json.dumps(line), flush=True)
+def bench_config(args):
+    """The workload both arms report (identical dicts)."""
+    return {"workload": WORKLOAD, "width": args.width, "height": args.height, "spp": args.spp, "output_spp": M}
 
 
 def main():
@@ -405,6 +437,7 @@ def main():
     total_ms = max_over_ranks(total_ms, dist)
     ms_per_step = total_ms / args.steps
     value = (world * Wd * Hd * args.steps / (total_ms / 1e3)) / 1e6
+    plain_host = out.cpu().numpy()          # the timed frame, for the parity check of cpu_baseline
 
     # learned routing: the same frame and timing with the router on, against the plain image
     routed = None
@@ -483,10 +516,10 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic scene, records resident in HBM)",
-        "config": {"workload": WORKLOAD, "width": Wd, "height": Hd, "spp": S, "output_spp": M,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (1.06 GB records, ~1 GB hierarchy)"},
+        "vs_baseline": None, "dtype": "f32", "data": DATA + ", records resident in HBM",
+        "config": bench_config(args),
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "l2": "inputs larger than L2 (1.06 GB records, ~1 GB hierarchy)",
         "build_ms": statistics.mean(b_ms), "query_kernel_ms": q_mean,
         "light_pass_ms": statistics.mean(l_ms), "heavy_pass_ms": statistics.mean(h_ms),
         "heavy_queries": sq.num_heavy_queries,
@@ -500,7 +533,8 @@ def main():
         "routed": routed, "batch": batch,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(rec, coc, args.cpu_rows, os.cpu_count() or 1)
+        line["cpu_baseline"] = cpu_baseline_sample(rec, coc, args.cpu_rows, os.cpu_count() or 1,
+                                                   gpu_img=plain_host)
     tg.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -4,7 +4,8 @@
 # for parity checks and the CPU baseline.  Test infrastructure only.
 #
 # The reference sources are compiled where they lie under the reference tree
-# (REF, default /root/reference); nothing is copied into the repository.  Five
+# (REF; by default the directory 'reference' beside the repository); nothing is
+# copied into the repository.  Five
 # headers need small portability edits for g++; the edited copies are generated
 # into oracle/_ref/gen/ (git-ignored) by the sed lines below:
 #   base/Array.hpp    explicit specialisations lack 'template<>' (Array.hpp:697-717)
@@ -22,7 +23,7 @@
 # so "reference output" means this build.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${REF:-/root/reference}"
+REF="${REF:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 SRC="$REF/src"
 if [ ! -d "$SRC/reconstruction_lib" ]; then
@@ -89,7 +90,13 @@ done
 # the driver sees private members (instrumentation only, see ref_driver.cpp)
 compile "$OUT/obj/m128/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$SRC/reconstruction_lib/reconstruction" & pids+=($!)
 compile "$OUT/obj/m64/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$OUT/gen_m64/reconstruction" & pids+=($!)
+# the seeded scene generator (the package's own host code, renamed), so that the
+# reference's CPU runs need no other library of this repository
+$CXX -std=c++17 -O2 -fPIC -ffp-contract=off -fno-fast-math -pthread -Dtlfr_synth_scene=ref_synth_scene \
+  -I"$HERE/../include" -c "$HERE/../temporal-lightfield-reconstruction_b200/csrc/synth_scene.cpp" \
+  -o "$OUT/obj/ref_synth_scene.o" & pids+=($!)
 for p in "${pids[@]}"; do wait "$p"; done
+objs+=("$OUT/obj/ref_synth_scene.o")
 
 $CXX -shared -pthread -o "$OUT/libtlfr_ref.so"     "${objs[@]}" "${m128[@]}" "$OUT/obj/m128/ref_driver.o"
 $CXX -shared -pthread -o "$OUT/libtlfr_ref_m64.so" "${objs[@]}" "${m64[@]}"  "$OUT/obj/m64/ref_driver.o"

@@ -60,3 +60,27 @@ def test_reference_arm_runs_on_rank0_only():
     with contextlib.redirect_stdout(buf):
         assert bench.run_reference(A(), 1, 2) is None
     assert buf.getvalue() == ""
+
+
+def test_reference_scene_generator_matches_package():
+    """The reference arm generates its inputs with the reference build's copy of
+    the scene generator (so it loads no library of the package); both copies
+    give the same records bit for bit."""
+    import numpy as np
+    import pytest
+    import tlfr
+    import bench
+    from tlfr_testutil import ref_available
+    if not ref_available():
+        pytest.skip("reference build absent")
+    a, ca = bench.ref_scene(40, 24, 4, 7)
+    b, cb = tlfr.synth_scene(bench.PRESET, 40, 24, 4, 7)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert tuple(np.float32(ca)) == tuple(np.float32(cb))
+
+
+def test_cpu_rows_spread_over_the_frame():
+    import bench
+    ys = bench.cpu_rows(1080, 8, 0)
+    assert len(ys) == 8 and ys == sorted(ys) and ys[0] < 135 and ys[-1] >= 945
+    assert bench.cpu_rows(1080, 8, 1) != ys
