@@ -361,6 +361,38 @@ def bench_config(args):
     return {"workload": WORKLOAD, "width": args.width, "height": args.height, "spp": args.spp, "output_spp": M}
 
 
+def run_profile_frame(args):
+    """One frame reconstructed from device-resident records: hierarchy build and
+    query passes timed with CUDA events per step (no CPU baseline, no router,
+    no batch).  Used for profiler captures of single kernels."""
+    import torch
+    import tlfr
+    torch.cuda.set_device(0)
+    Wd, Hd, S = args.width, args.height, args.spp
+    rec, coc = tlfr.synth_scene(args.scene, Wd, Hd, S, 2)
+    d_rec = torch.from_numpy(rec).cuda()
+    stream = torch.cuda.current_stream()
+    tg = tlfr.TreeGather(None, tlfr.CameraParams(device=0), stream=stream.cuda_stream,
+                         device_records=(d_rec.data_ptr(), (Wd, Hd, S), coc))
+    out = torch.empty((Hd, Wd, 4), dtype=torch.float32, device="cuda")
+    rows = []
+    for k in range(args.warmup + args.steps):
+        tg.rebuild(d_rec.data_ptr())
+        b = tg.stats().build_ms
+        tg.reconstruct_to_device(out.data_ptr())
+        st = tg.stats()
+        if k >= args.warmup:
+            rows.append((b, st.light_ms, st.heavy_ms, st.query_kernel_ms, st.num_heavy_queries))
+    torch.cuda.synchronize()
+    med = lambda i: statistics.median(r[i] for r in rows)
+    line = {"profile_frame": f"{Wd}x{Hd}x{S}", "scene": args.scene, "steps": args.steps, "warmup": args.warmup,
+            "build_ms": med(0), "light_ms": med(1), "heavy_ms": med(2), "query_kernel_ms": med(3),
+            "heavy_queries": int(rows[-1][4]), "output_samples": Wd * Hd * M,
+            "checksum": float(out.double().sum().item())}
+    tg.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.profile_frame:
