@@ -1120,7 +1120,6 @@ struct CoopScratch
 {
     Leaf    leaves[32][kCLeaf];
     RSample rs[kCRs];
-    float4  prod[kCRs];
     Surf    surf[kCSurf];
 };
 
@@ -1191,8 +1190,15 @@ __device__ int traverse_sorted(const QParams& P, const Query& o, float R, Leaf* 
 }
 
 // Cooperative collectInputSamples2 scan (RO.cpp:412-503) over sorted leaves.
-// All lanes call it with the same arguments; returns the accepted count (same
-// on all lanes) or -1 when rs / surf outgrow the scratch.
+// The leaves are taken 32 at a time: lane k holds leaf g+k's sample range, and
+// the group's samples are scanned as one flat sequence in chunks of 32 that
+// span leaf boundaries (as in the light pass).  A chunk's accepted samples are
+// handled leaf by leaf in order: sameSurface at the leaf's first accepted
+// sample against every leaf since the open surface began (lanes over those
+// leaves), then the samples appended to rs in sample order with the surface's
+// quadrant mask and first strict minimum.  All lanes call it with the same
+// arguments; returns the accepted count (same on all lanes) or -1 when rs /
+// surf outgrow the scratch.
 __device__ int coop_scan(const QParams& P, const Query& o, float R, const Leaf* leaves, int nleaves,
                          CoopScratch& S, int& nsurf_out)
 {
@@ -1201,80 +1207,111 @@ __device__ int coop_scan(const QParams& P, const Query& o, float R, const Leaf* 
     const float uvtmin[3] = { o.u - RANGE, o.v - RANGE, o.t - 0.5f * RANGE };
     const float uvtmax[3] = { o.u + RANGE, o.v + RANGE, o.t + 0.5f * RANGE };
     const float R2 = R * R;
-    int nsurf = 0, nrs = 0, surfaceStart = 0;
+    int nsurf = 0, nrs = 0, surfaceStart = 0, last_leaf = -1;
     // the open surface's running state, identical on all lanes
     float minDist = kF32Max;
     int minIndex = -1, quad = 0, sstart = 0;
-    for (int lidx = 0; lidx < nleaves; lidx++)
+    for (int g = 0; g < nleaves; g += 32)
     {
-        const QNode node = load_node(P.nodes, leaves[lidx].node);
-        const int s0 = node.d.z, s1 = node.d.w;
-        bool first = true;
-        for (int base = s0; base < s1; base += 32)
+        const int ng = mini(32, nleaves - g);
+        int my_s0 = 0, my_n = 0;
+        if (lane < ng)
         {
-            const int i = base + lane;
+            const int4 d = P.nodes[leaves[g + lane].node].d;
+            my_s0 = d.z;
+            my_n = d.w - d.z;
+        }
+        int my_f = my_n;
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            const int v = __shfl_up_sync(0xffffffffu, my_f, off);
+            if (lane >= off)
+                my_f += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, my_f, 31);
+        my_f -= my_n;
+        for (int base = 0; base < total; base += 32)
+        {
+            // leaf (within the group) and sample of flat index base + lane; every
+            // leaf holds at least one sample, so leaf starts are distinct
+            const bool starts_in = lane < ng && my_f > base && my_f < base + 32;
+            const unsigned starts = __reduce_or_sync(0xffffffffu, starts_in ? 1u << (my_f - base) : 0u);
+            const int k = __popc(__ballot_sync(0xffffffffu, lane < ng && my_f <= base)) - 1 +
+                          __popc(starts & ((2u << lane) - 1u));
+            const int i = __shfl_sync(0xffffffffu, my_s0, k & 31) + (base + lane - __shfl_sync(0xffffffffu, my_f, k & 31));
             float x = 0, y = 0, d2 = 0;
             bool acc = false;
-            if (i < s1)
+            if (base + lane < total)
             {
                 d2 = reproject(P, i, o, x, y);
                 acc = d2 <= R2;
             }
-            const unsigned m = __ballot_sync(0xffffffffu, acc);
-            if (!m)
+            unsigned accm = __ballot_sync(0xffffffffu, acc);
+            if (!accm)
                 continue;
-            if (first)
-            {
-                first = false;
-                bool same = true;
-                for (int jb = surfaceStart; jb < lidx && same; jb += 32)
-                {
-                    const int j = jb + lane;
-                    const bool ok = (j < lidx) ? same_surface(node, load_node(P.nodes, leaves[j].node), uvtmin, uvtmax) : true;
-                    same = __all_sync(0xffffffffu, ok);
-                }
-                if (!same || nsurf == 0)
-                {
-                    if (nsurf > 0 && lane == 0)
-                    {
-                        Surf& p = S.surf[nsurf - 1];
-                        p.n = nrs - sstart; p.minDist = minDist; p.minIndex = minIndex; p.quad = quad;
-                    }
-                    if (nsurf == kCSurf)
-                        return -1;
-                    surfaceStart = lidx;
-                    nsurf++;
-                    sstart = nrs;
-                    minDist = kF32Max; minIndex = -1; quad = 0;
-                    if (lane == 0) S.surf[nsurf - 1].start = nrs;
-                }
-            }
-            const int cnt = __popc(m);
-            if (nrs + cnt > kCRs)
-                return -1;
-            const int pos = nrs + __popc(m & lanes_below(lane));
             const float dx = x - o.x, dy = y - o.y;
             const int rpos = (dx >= 0 ? 1 : 4) | (dy >= 0 ? 2 : 8);
-            if (acc)
-            {
-                RSample r;
-                r.x = x; r.y = y; r.index = i; r.rpos = rpos;
-                S.rs[pos] = r;
-            }
-            quad |= __reduce_or_sync(0xffffffffu, acc ? (1 << (rpos & 3)) : 0);
-            // first strict minimum in acceptance order (RO.cpp:494-499)
             const float dist = acc ? sqrtf(d2) : kF32Max;
-            float cmin = dist;
-            for (int off = 16; off > 0; off >>= 1)
-                cmin = minr(cmin, __shfl_xor_sync(0xffffffffu, cmin, off));
-            if (cmin < minDist)
+            while (accm)
             {
-                const unsigned at = __ballot_sync(0xffffffffu, acc && dist == cmin);
-                const int fl = __ffs(at) - 1;
-                minDist = cmin;
-                minIndex = nrs + __popc(m & lanes_below(fl)) - sstart;
+                const int kseg = __shfl_sync(0xffffffffu, k, __ffs(accm) - 1);
+                const unsigned m = accm & __ballot_sync(0xffffffffu, k == kseg);
+                accm &= ~m;
+                const int lidx = g + kseg;
+                if (lidx != last_leaf)
+                {
+                    // first accepted sample of this leaf
+                    last_leaf = lidx;
+                    bool same = true;
+                    if (nsurf > 0)
+                    {
+                        const QNode node = load_node(P.nodes, leaves[lidx].node);
+                        for (int jb = surfaceStart; jb < lidx && same; jb += 32)
+                        {
+                            const int j = jb + lane;
+                            const bool ok = (j < lidx) ? same_surface(node, load_node(P.nodes, leaves[j].node), uvtmin, uvtmax) : true;
+                            same = __all_sync(0xffffffffu, ok);
+                        }
+                    }
+                    if (!same || nsurf == 0)
+                    {
+                        if (nsurf > 0 && lane == 0)
+                        {
+                            Surf& p = S.surf[nsurf - 1];
+                            p.n = nrs - sstart; p.minDist = minDist; p.minIndex = minIndex; p.quad = quad;
+                        }
+                        if (nsurf == kCSurf)
+                            return -1;
+                        surfaceStart = lidx;
+                        nsurf++;
+                        sstart = nrs;
+                        minDist = kF32Max; minIndex = -1; quad = 0;
+                        if (lane == 0) S.surf[nsurf - 1].start = nrs;
+                    }
+                }
+                const int cnt = __popc(m);
+                if (nrs + cnt > kCRs)
+                    return -1;
+                const bool mine = (m >> lane) & 1u;
+                if (mine)
+                {
+                    RSample r;
+                    r.x = x; r.y = y; r.index = i; r.rpos = rpos;
+                    S.rs[nrs + __popc(m & lanes_below(lane))] = r;
+                }
+                quad |= __reduce_or_sync(0xffffffffu, mine ? (1 << (rpos & 3)) : 0);
+                // first strict minimum in acceptance order (RO.cpp:494-499);
+                // distances are non-negative, so their bits order as integers
+                const unsigned dbits = mine ? __float_as_uint(dist) : 0x7f800000u;
+                const unsigned mbits = __reduce_min_sync(0xffffffffu, dbits);
+                if (__uint_as_float(mbits) < minDist)
+                {
+                    const int fl = __ffs(__ballot_sync(0xffffffffu, mine && dbits == mbits)) - 1;
+                    minDist = __uint_as_float(mbits);
+                    minIndex = nrs + __popc(m & lanes_below(fl)) - sstart;
+                }
+                nrs += cnt;
             }
-            nrs += cnt;
         }
     }
     if (nsurf > 0 && lane == 0)
@@ -1300,59 +1337,116 @@ __device__ __forceinline__ void coop_reverse(RSample* a, int lo, int hi)     // 
     __syncwarp();
 }
 
-// Moves (m, k) forward by step pairs in the m-major order of pairs
-// m < k <= n-2; m > n-3 afterwards means past the last pair.
-__device__ __forceinline__ void pair_advance(int n, int step, int& m, int& k)
-{
-    k += step;
-    while (m <= n - 3 && k > n - 2)
-    {
-        const int over = k - (n - 1);
-        m++;
-        k = m + 1 + over;
-    }
-}
+// Coverage test of one surface (RO.cpp:221-259): is there a triangle of three
+// of its samples m < k < l that together hold all four quadrant bits, whose
+// sides are at most 2*dispersion long, with a vertex within dispersion of the
+// output sample, and that contains the output sample (double-precision edge
+// functions)?  Any such triangle settles it, so the search order does not
+// change the answer.  The pairwise side test is computed once as an adjacency
+// bit matrix in shared memory (bit l of row m: m < l, |r_m - r_l| <= 2R), with
+// bit masks of the samples within R and of each quadrant pattern; the third
+// vertices of a pair (m, k) are then the set bits of row m & row k & the masks
+// that complete the quadrants and the within-R condition, and only those reach
+// the edge functions.  Lanes take the pairs (m, k), k over the lanes.
+constexpr int kTriMax = 200;                    // n >= 200 is accepted without the search (RO.cpp:215)
+constexpr int kTriWords = (kTriMax + 31) / 32;
 
-// Any triangle of rs[0..n) covering o (RO.cpp:221-259), searched by all lanes:
-// lane l takes pairs l, l+32, ... and the third vertices after each.
-__device__ bool coop_triangle(const RSample* in, int n, const Query& o, float dispersion)
+struct TriShared
+{
+    unsigned adj[kTriMax * kTriWords];
+    unsigned mask[5 * kTriWords];               // quadrant patterns 3, 6, 9, 12; within R
+};
+
+__device__ bool coop_triangle(const RSample* in, int n, const Query& o, float dispersion, TriShared& T)
 {
     const int lane = threadIdx.x & 31;
-    const int pairs = (n - 2) * (n - 1) / 2;
-    bool found = false;
-    int m = 0, k = 1;
-    pair_advance(n, lane, m, k);
-    for (int pb = 0; pb < pairs; pb += 32, pair_advance(n, 32, m, k))
+    const int W = (n + 31) >> 5;
+    const float side = 2 * dispersion;
+    for (int w = 0; w < W; w++)
     {
-        if (m <= n - 3)
+        const int i = (w << 5) + lane;
+        const bool v = i < n;
+        RSample r{};
+        if (v)
+            r = in[i];
+        const bool near = v && !(len2(r.x - o.x, r.y - o.y) > dispersion);
+        const unsigned q3 = __ballot_sync(0xffffffffu, v && r.rpos == 3);
+        const unsigned q6 = __ballot_sync(0xffffffffu, v && r.rpos == 6);
+        const unsigned q9 = __ballot_sync(0xffffffffu, v && r.rpos == 9);
+        const unsigned q12 = __ballot_sync(0xffffffffu, v && r.rpos == 12);
+        const unsigned nr = __ballot_sync(0xffffffffu, near);
+        if (lane == 0)
         {
-            const RSample r0 = in[m], r1 = in[k];
-            const int rp01 = r0.rpos | r1.rpos;
-            if (!(len2(r0.x - r1.x, r0.y - r1.y) > 2 * dispersion))
+            T.mask[0 * kTriWords + w] = q3; T.mask[1 * kTriWords + w] = q6;
+            T.mask[2 * kTriWords + w] = q9; T.mask[3 * kTriWords + w] = q12;
+            T.mask[4 * kTriWords + w] = nr;
+        }
+    }
+    for (int m = 0; m < n - 1; m++)
+    {
+        const RSample rm = in[m];
+        for (int w = (m + 1) >> 5; w < W; w++)
+        {
+            const int k = (w << 5) + lane;
+            bool b = false;
+            if (k > m && k < n)
             {
-                for (int l = k + 1; l < n && !found; l++)
+                const RSample rk = in[k];
+                b = !(len2(rm.x - rk.x, rm.y - rk.y) > side);
+            }
+            const unsigned bits = __ballot_sync(0xffffffffu, b);
+            if (lane == 0)
+                T.adj[m * kTriWords + w] = bits;
+        }
+    }
+    __syncwarp();
+    for (int m = 0; m < n - 2; m++)
+    {
+        const RSample r0 = in[m];
+        const bool near0 = (T.mask[4 * kTriWords + (m >> 5)] >> (m & 31)) & 1u;
+        for (int kb = m + 1; kb < n - 1; kb += 32)
+        {
+            const int k = kb + lane;
+            bool found = false;
+            if (k < n - 1 && ((T.adj[m * kTriWords + (k >> 5)] >> (k & 31)) & 1u))
+            {
+                const RSample r1 = in[k];
+                const int missing = 15 & ~(r0.rpos | r1.rpos);
+                const bool nearpair = near0 || ((T.mask[4 * kTriWords + (k >> 5)] >> (k & 31)) & 1u);
+                for (int w = k >> 5; w < W && !found; w++)
                 {
-                    const RSample r2 = in[l];
-                    if ((rp01 | r2.rpos) != 15)
-                        continue;
-                    if (len2(r0.x - r2.x, r0.y - r2.y) > 2 * dispersion ||
-                        len2(r1.x - r2.x, r1.y - r2.y) > 2 * dispersion)
-                        continue;
-                    if (len2(r0.x - o.x, r0.y - o.y) > dispersion && len2(r1.x - o.x, r1.y - o.y) > dispersion &&
-                        len2(r2.x - o.x, r2.y - o.y) > dispersion)
-                        continue;
-                    EdgeFn e0 = edge_make(r1.x, r1.y, r2.x, r2.y);
-                    EdgeFn e1 = edge_make(r2.x, r2.y, r0.x, r0.y);
-                    EdgeFn e2 = edge_make(r0.x, r0.y, r1.x, r1.y);
-                    bool p0 = edge_test(e0, o.x, o.y);
-                    bool p1 = edge_test(e1, o.x, o.y);
-                    bool p2 = edge_test(e2, o.x, o.y);
-                    found = (p0 && p1 && p2) || (!p0 && !p1 && !p2);
+                    unsigned c = T.adj[m * kTriWords + w] & T.adj[k * kTriWords + w];
+                    if (w == (k >> 5))
+                        c &= ~((2u << (k & 31)) - 1u);          // third vertices l > k
+                    if (missing)
+                    {
+                        unsigned q = 0;
+                        if ((3 & missing) == missing) q |= T.mask[0 * kTriWords + w];
+                        if ((6 & missing) == missing) q |= T.mask[1 * kTriWords + w];
+                        if ((9 & missing) == missing) q |= T.mask[2 * kTriWords + w];
+                        if ((12 & missing) == missing) q |= T.mask[3 * kTriWords + w];
+                        c &= q;
+                    }
+                    if (!nearpair)
+                        c &= T.mask[4 * kTriWords + w];
+                    while (c && !found)
+                    {
+                        const int l = (w << 5) + __ffs(c) - 1;
+                        c &= c - 1;
+                        const RSample r2 = in[l];
+                        EdgeFn e0 = edge_make(r1.x, r1.y, r2.x, r2.y);
+                        EdgeFn e1 = edge_make(r2.x, r2.y, r0.x, r0.y);
+                        EdgeFn e2 = edge_make(r0.x, r0.y, r1.x, r1.y);
+                        bool p0 = edge_test(e0, o.x, o.y);
+                        bool p1 = edge_test(e1, o.x, o.y);
+                        bool p2 = edge_test(e2, o.x, o.y);
+                        found = (p0 && p1 && p2) || (!p0 && !p1 && !p2);
+                    }
                 }
             }
+            if (__any_sync(0xffffffffu, found))
+                return true;
         }
-        if (__any_sync(0xffffffffu, found))
-            return true;
     }
     return false;
 }
@@ -1362,10 +1456,12 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
              float4* __restrict__ qcol, int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap,
              CoopScratch* __restrict__ scratch)
 {
+    __shared__ TriShared sh_tri[kCWarps];
     const int lane = threadIdx.x & 31;
     const int warp = blockIdx.x * kCWarps + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * kCWarps;
     CoopScratch& S = scratch[warp];
+    TriShared& T = sh_tri[threadIdx.x >> 5];
     const int n = *queue_count;
     for (int b = warp * 32; b < n; b += nwarps * 32)
     {
@@ -1491,40 +1587,43 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
                 }
                 if (!fetch2R || sf.minDist < 0.f || sidx == nsurf - 1)
                     found = true;
-                if (cnt >= 200)
+                if (cnt >= kTriMax)
                     found = true;
-                if (!found)
-                    found = coop_triangle(in, cnt, o, dispersion);
+                if (!found && cnt >= 3)
+                    found = coop_triangle(in, cnt, o, dispersion, T);
                 if (found)
                 {
-                    for (int k = lane; k < cnt; k += 32)
+                    // tent filter (RO.cpp:274-294): products in parallel, summed
+                    // in sample order by every lane from shuffles
+                    res = make_float4(0, 0, 0, 0);
+                    for (int kb = 0; kb < cnt; kb += 32)
                     {
-                        const RSample r = in[k];
-                        const float dx = o.x - r.x, dy = o.y - r.y;
-                        const float weight = 1 - len2(dx, dy) / dispersion;
-                        // alpha is 1 (forced at load), so an included sample has pr.w = weight > 0;
-                        // pr.w = -1 marks a sample the reference skips (weight <= 0)
-                        float4 pr = make_float4(0, 0, 0, -1.0f);
-                        if (weight > 0)
+                        const int k = kb + lane;
+                        float4 pr = make_float4(0, 0, 0, 0);
+                        bool inc = false;
+                        if (k < cnt)
                         {
-                            const float4 c = P.s_col[r.index];
-                            pr = make_float4(c.x * weight, c.y * weight, c.z * weight, c.w * weight);
+                            const RSample r = in[k];
+                            const float dx = o.x - r.x, dy = o.y - r.y;
+                            const float weight = 1 - len2(dx, dy) / dispersion;
+                            if (weight > 0)
+                            {
+                                const float4 c = P.s_col[r.index];
+                                pr = make_float4(c.x * weight, c.y * weight, c.z * weight, c.w * weight);
+                                inc = true;
+                            }
                         }
-                        S.prod[k] = pr;
-                    }
-                    __syncwarp();
-                    if (lane == 0)
-                    {
-                        for (int k = 0; k < cnt; k++)
+                        for (unsigned mi = __ballot_sync(0xffffffffu, inc); mi; mi &= mi - 1)
                         {
-                            const float4 pr = S.prod[k];
-                            if (pr.w < 0)
-                                continue;
-                            res.x += pr.x; res.y += pr.y; res.z += pr.z; res.w += pr.w;
+                            const int src = __ffs(mi) - 1;
+                            res.x += __shfl_sync(0xffffffffu, pr.x, src);
+                            res.y += __shfl_sync(0xffffffffu, pr.y, src);
+                            res.z += __shfl_sync(0xffffffffu, pr.z, src);
+                            res.w += __shfl_sync(0xffffffffu, pr.w, src);
                         }
-                        const float oow = rcp(res.w);
-                        res.x *= oow; res.y *= oow; res.z *= oow; res.w *= oow;
                     }
+                    const float oow = rcp(res.w);
+                    res.x *= oow; res.y *= oow; res.z *= oow; res.w *= oow;
                     nearS = sidx; nearI = sf.minIndex;
                 }
             }
