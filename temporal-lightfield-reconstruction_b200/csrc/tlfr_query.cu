@@ -547,9 +547,10 @@ __device__ void flush_stats(const QStats& st, DevStats* ds)
 constexpr int kBlock = 128;
 // capacities of the full per-query path (statistics pass and heavy pass)
 constexpr int kStackCap = 96, kLeafCap = 256, kRsCap = 512, kSurfCap = 64;
-// capacities of the light pass: traversal stack and leaf list per output
-// sample, both in shared memory
-constexpr int kLStack = 16, kLLeaf = 32;
+// capacities of the light pass, both in shared memory: the warp's traversal
+// stack (the union depth-first walk keeps at most one waiting sibling per level
+// of the hierarchy) and the leaf list per output sample
+constexpr int kLStack = 64, kLLeaf = 32;
 
 // Per-thread column of a shared-memory array laid out [slot][thread]: a warp
 // whose lanes touch different slots still hits distinct banks.  The host build
@@ -605,81 +606,109 @@ TLFR_HD bool leaf_append(const QParams& P, const Query& o, const Column<float2>&
     return true;
 }
 
-// collectInputSamples2's traversal and leaf sort (RO.cpp:368-407) for one output
-// sample at radius R: DFS in the reference's order (push child0, child1, pop the
-// last) into the leaf column, then FW::sort of the leaves by key.  Children are
-// stored as pairs, so a node that intersects has both children loaded and
-// tested together and only those that intersect are pushed (a leaf child waits
-// on the stack only behind an internal child1).  The loop has no early exit (an
-// overflow sets a flag), so a warp reconverges at the end of every step.
-// Returns the leaf count, or -1 when the stack or the leaf column is full.
-TLFR_HD int collect_pairs(const QParams& P, const Column<int>& stack, int stack_cap, const Column<float2>& leaves,
-                          int leaf_cap, const Query& o, float R)
+// collectInputSamples2's traversal and leaf sort (RO.cpp:368-407) at radius R
+// for the warp's 32 output samples together.  The warp walks the union of the
+// nodes its lanes reach, depth first in the reference's order (push child0,
+// child1, pop the last); every stack entry carries the lanes for which all the
+// entry's ancestors intersected.  Children are stored as pairs, so a popped
+// entry loads both children once for the whole warp (one address for all
+// lanes) and each lane tests them against its own output sample.  Restricted
+// to the nodes one lane reaches, this order is that lane's own depth-first
+// order, so each lane's leaf column receives its leaves in the order the
+// reference's traversal finds them; FW::sort then orders them by key.  The
+// stack (wcap entries of node, lane mask) is shared by the warp.  All 32 lanes
+// call it; lanes with active false take no part.  Returns the lane's leaf
+// count, or -1 when its leaf column is full or the warp's stack is.
+__device__ int collect_packet(const QParams& P, int2* wstack, int wcap, const Column<float2>& leaves, int leaf_cap,
+                              const Query& o, float R, bool active)
 {
+    const int lane = threadIdx.x & 31;
     int nleaves = 0, sp = 0;
-    bool ok = true;
+    bool ok = true, wfull = false;
     {
         const QNode rn = load_node(P.nodes, P.root);
-        if (node_intersect(rn, o, R))
+        const bool h = active && node_intersect(rn, o, R);
+        const unsigned m = __ballot_sync(0xffffffffu, h);
+        if (rn.d.x < 0)
         {
-            if (rn.d.x < 0)
+            if (h)
                 ok = leaf_append(P, o, leaves, leaf_cap, nleaves, P.root, rn.d.z);
-            else
-                stack[sp++] = rn.d.x;
+        }
+        else if (m)
+        {
+            if (lane == 0)
+                wstack[0] = make_int2(rn.d.x, (int)m);
+            sp = 1;
         }
     }
-    // stack entries: >= 0 the first child of an intersecting internal node;
-    // < 0 (~node) an intersecting leaf
-    while (sp > 0 && ok)
+    __syncwarp();
+    // entries: x >= 0 the first child of a pair whose parent intersected; x < 0
+    // (~node) a leaf that intersected, waiting behind its internal sibling
+    while (sp > 0)
     {
-        const int e = stack[--sp];
-        if (e < 0)
-            ok = leaf_append(P, o, leaves, leaf_cap, nleaves, ~e, P.nodes[~e].d.z);
+        const int2 e = wstack[--sp];
+        const bool in = ((unsigned)e.y >> lane) & 1u;
+        if (e.x < 0)
+        {
+            if (in && ok)
+                ok = leaf_append(P, o, leaves, leaf_cap, nleaves, ~e.x, P.nodes[~e.x].d.z);
+            continue;
+        }
+        const QNode n0 = load_node(P.nodes, e.x);
+        const QNode n1 = load_node(P.nodes, e.x + 1);
+        const bool h0 = in && node_intersect(n0, o, R);
+        const bool h1 = in && node_intersect(n1, o, R);
+        const unsigned m0 = __ballot_sync(0xffffffffu, h0);
+        const unsigned m1 = __ballot_sync(0xffffffffu, h1);
+        if (m1 && n1.d.x >= 0)
+        {
+            // child1's subtree comes first; child0 waits below it
+            const int np = m0 ? 2 : 1;
+            if (sp + np > wcap)
+            {
+                wfull = true;
+                break;
+            }
+            if (lane == 0)
+            {
+                if (m0)
+                    wstack[sp] = make_int2(n0.d.x >= 0 ? n0.d.x : ~e.x, (int)m0);
+                wstack[sp + np - 1] = make_int2(n1.d.x, (int)m1);
+            }
+            sp += np;
+        }
         else
         {
-            const QNode n0 = load_node(P.nodes, e);
-            const QNode n1 = load_node(P.nodes, e + 1);
-            const bool h0 = node_intersect(n0, o, R);
-            const bool h1 = node_intersect(n1, o, R);
-            if (h1 && n1.d.x >= 0)
+            if (h1 && ok)
+                ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e.x + 1, n1.d.z);
+            if (m0)
             {
-                // child1's subtree comes first; child0 waits below it
-                if (sp + 2 > stack_cap)
-                    ok = false;
+                if (n0.d.x < 0)
+                {
+                    if (h0 && ok)
+                        ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e.x, n0.d.z);
+                }
+                else if (sp + 1 > wcap)
+                {
+                    wfull = true;
+                    break;
+                }
                 else
                 {
-                    if (h0)
-                        stack[sp++] = n0.d.x >= 0 ? n0.d.x : ~e;
-                    stack[sp++] = n1.d.x;
-                }
-            }
-            else
-            {
-                if (h1)
-                    ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e + 1, n1.d.z);
-                if (h0 && ok)
-                {
-                    if (n0.d.x < 0)
-                        ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e, n0.d.z);
-                    else if (sp + 1 > stack_cap)
-                        ok = false;
-                    else
-                        stack[sp++] = n0.d.x;
+                    if (lane == 0)
+                        wstack[sp] = make_int2(n0.d.x, (int)m0);
+                    sp++;
                 }
             }
         }
+        __syncwarp();
     }
-    if (!ok)
+    __syncwarp();
+    if (wfull || !ok)
         return -1;
     LLeafSort ls{ leaves };
     fw_sort(ls, 0, nleaves);
     return nleaves;
-}
-
-// Light pass, part 1: each lane collects its own output sample's leaves at 1R.
-TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Column<float2>& leaves, const Query& o)
-{
-    return collect_pairs(P, stack, kLStack, leaves, kLLeaf, o, P.disp0);
 }
 
 // Light pass, part 2 (RO.cpp:94-99, 165-304 for the common case): the 1R scan
@@ -1016,10 +1045,10 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
               int* __restrict__ heavy_count)
 {
     __shared__ float2 sh_leaves[kLLeaf][kBlock];
-    __shared__ int sh_stack[kLStack][kBlock];
+    __shared__ int2 sh_stack[kBlock / 32][kLStack];
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
-    const Column<int> stack{ &sh_stack[0][threadIdx.x], kBlock };
+    int2* wstack = sh_stack[threadIdx.x >> 5];
     for (long long u = blockIdx.x; u < L.units; u += gridDim.x)
     {
         // each lane: traversal and leaf sort of its own output sample
@@ -1030,11 +1059,12 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
         const long long pix = valid ? (PROBE ? q / kProbe : q / P.M) : 0;
         const bool fast = !PROBE && valid && P.route_fast && P.route_fast[pix];
         if (valid)
-        {
             o = PROBE ? make_query(P, (int)(pix % P.W), (int)(pix / P.W), (int)((q % kProbe) * P.M / kProbe))
                       : query_of(P, q);
-            nl = light_collect(P, stack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, o);
-        }
+        nl = collect_packet(P, wstack, kLStack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, kLLeaf, o,
+                            P.disp0, valid);
+        if (!valid)
+            nl = -2;
         const unsigned fast_lanes = __ballot_sync(0xffffffffu, fast);
         __syncwarp();
         // the warp: the 1R scan of each lane's output sample in turn
@@ -1105,10 +1135,10 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
 // ---------------------------------------------------------------------------
 constexpr int kCWarps = 4;
 // blocks of the cooperative full-path pass (its working lists are per warp):
-// 8 per SM with registers capped to fit (64) measured 5% faster than 6 and 26%
-// faster than 4
+// 5 per SM leave it its 89 registers without spills; at 1920x1080x8 it measured
+// 563 ms against 651 ms at 6 (80 registers, spills) and 699 ms at 8 (64)
 #ifndef TLFR_COOP_BLOCKS_PER_SM
-#define TLFR_COOP_BLOCKS_PER_SM 8
+#define TLFR_COOP_BLOCKS_PER_SM 5
 #endif
 constexpr int kCoopBlocksPerSM = TLFR_COOP_BLOCKS_PER_SM;
 constexpr int kCLeaf = 256;         // leaves per lane's traversal
@@ -1342,19 +1372,19 @@ __device__ __forceinline__ void coop_reverse(RSample* a, int lo, int hi)     // 
 // sides are at most 2*dispersion long, with a vertex within dispersion of the
 // output sample, and that contains the output sample (double-precision edge
 // functions)?  Any such triangle settles it, so the search order does not
-// change the answer.  The pairwise side test is computed once as an adjacency
-// bit matrix in shared memory (bit l of row m: m < l, |r_m - r_l| <= 2R), with
-// bit masks of the samples within R and of each quadrant pattern; the third
-// vertices of a pair (m, k) are then the set bits of row m & row k & the masks
-// that complete the quadrants and the within-R condition, and only those reach
-// the edge functions.  Lanes take the pairs (m, k), k over the lanes.
+// change the answer.  For each first vertex m the warp builds one bit row: the
+// samples l > m within 2*dispersion of m; lanes then take the second vertices
+// k of that row, and the third vertices of (m, k) are the set bits of the row
+// beyond k that complete the quadrants (bit masks per quadrant pattern) and the
+// within-dispersion condition (a bit mask), each checked against k's side
+// length before the edge functions.
 constexpr int kTriMax = 200;                    // n >= 200 is accepted without the search (RO.cpp:215)
 constexpr int kTriWords = (kTriMax + 31) / 32;
 
 struct TriShared
 {
-    unsigned adj[kTriMax * kTriWords];
-    unsigned mask[5 * kTriWords];               // quadrant patterns 3, 6, 9, 12; within R
+    unsigned row[kTriWords];                    // samples l > m within 2*dispersion of m
+    unsigned mask[5 * kTriWords];               // quadrant patterns 3, 6, 9, 12; within dispersion
 };
 
 __device__ bool coop_triangle(const RSample* in, int n, const Query& o, float dispersion, TriShared& T)
@@ -1382,9 +1412,9 @@ __device__ bool coop_triangle(const RSample* in, int n, const Query& o, float di
             T.mask[4 * kTriWords + w] = nr;
         }
     }
-    for (int m = 0; m < n - 1; m++)
+    for (int m = 0; m < n - 2; m++)
     {
-        const RSample rm = in[m];
+        const RSample r0 = in[m];
         for (int w = (m + 1) >> 5; w < W; w++)
         {
             const int k = (w << 5) + lane;
@@ -1392,30 +1422,26 @@ __device__ bool coop_triangle(const RSample* in, int n, const Query& o, float di
             if (k > m && k < n)
             {
                 const RSample rk = in[k];
-                b = !(len2(rm.x - rk.x, rm.y - rk.y) > side);
+                b = !(len2(r0.x - rk.x, r0.y - rk.y) > side);
             }
             const unsigned bits = __ballot_sync(0xffffffffu, b);
             if (lane == 0)
-                T.adj[m * kTriWords + w] = bits;
+                T.row[w] = bits;
         }
-    }
-    __syncwarp();
-    for (int m = 0; m < n - 2; m++)
-    {
-        const RSample r0 = in[m];
+        __syncwarp();
         const bool near0 = (T.mask[4 * kTriWords + (m >> 5)] >> (m & 31)) & 1u;
         for (int kb = m + 1; kb < n - 1; kb += 32)
         {
             const int k = kb + lane;
             bool found = false;
-            if (k < n - 1 && ((T.adj[m * kTriWords + (k >> 5)] >> (k & 31)) & 1u))
+            if (k < n - 1 && ((T.row[k >> 5] >> (k & 31)) & 1u))
             {
                 const RSample r1 = in[k];
                 const int missing = 15 & ~(r0.rpos | r1.rpos);
                 const bool nearpair = near0 || ((T.mask[4 * kTriWords + (k >> 5)] >> (k & 31)) & 1u);
                 for (int w = k >> 5; w < W && !found; w++)
                 {
-                    unsigned c = T.adj[m * kTriWords + w] & T.adj[k * kTriWords + w];
+                    unsigned c = T.row[w];
                     if (w == (k >> 5))
                         c &= ~((2u << (k & 31)) - 1u);          // third vertices l > k
                     if (missing)
@@ -1434,6 +1460,8 @@ __device__ bool coop_triangle(const RSample* in, int n, const Query& o, float di
                         const int l = (w << 5) + __ffs(c) - 1;
                         c &= c - 1;
                         const RSample r2 = in[l];
+                        if (len2(r1.x - r2.x, r1.y - r2.y) > side)
+                            continue;
                         EdgeFn e0 = edge_make(r1.x, r1.y, r2.x, r2.y);
                         EdgeFn e1 = edge_make(r2.x, r2.y, r0.x, r0.y);
                         EdgeFn e2 = edge_make(r0.x, r0.y, r1.x, r1.y);
@@ -1447,6 +1475,7 @@ __device__ bool coop_triangle(const RSample* in, int n, const Query& o, float di
             if (__any_sync(0xffffffffu, found))
                 return true;
         }
+        __syncwarp();       // the next row overwrites T.row
     }
     return false;
 }
@@ -1469,18 +1498,31 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
         // pass found to need it, at 1R for those that outgrew the light pass's
         // capacities (they start over from the 1R fetch)
         const int entry = (b + lane < n) ? queue[b + lane] : -1;
-        const bool restart = entry >= 0 && (entry & kQueueRestart);
+        bool restart = entry >= 0 && (entry & kQueueRestart);
         const bool valid = entry >= 0;
         const int myq = valid ? (entry & ~kQueueRestart) : 0;
         Query myo = query_of(P, myq);
         int mycount = valid ? traverse_sorted(P, myo, restart ? P.disp0 : P.disp0 * 2, S.leaves[lane], kCLeaf) : 0;
         __syncwarp();
-        // 2. each sample of the batch by the whole warp
-        for (int j = 0; j < 32; j++)
+        // 2. each sample of the batch by the whole warp.  A restarted sample whose
+        // 1R fetch ends with fetch2R true is set aside; its lane traverses at 2R
+        // (all such lanes in parallel) and it runs again in a second round.
+        unsigned todo = __ballot_sync(0xffffffffu, valid);
+        for (int round = 0; round < 2 && todo; round++)
         {
-            const bool vj = __shfl_sync(0xffffffffu, valid, j);
-            if (!vj)
-                continue;
+        if (round == 1)
+        {
+            if ((todo >> lane) & 1u)
+            {
+                mycount = traverse_sorted(P, myo, P.disp0 * 2, S.leaves[lane], kCLeaf);
+                restart = false;
+            }
+            __syncwarp();
+        }
+        unsigned redo = 0;
+        for (unsigned jm = todo; jm; jm &= jm - 1)
+        {
+            const int j = __ffs(jm) - 1;
             const int qj = __shfl_sync(0xffffffffu, myq, j);
             int nl = __shfl_sync(0xffffffffu, mycount, j);
             bool ovf = nl < 0;
@@ -1502,12 +1544,8 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
                     fetch2R = nsurf == 0 || (S.surf[0].quad != 0xF && nsurf > 1);
                 if (!ovf && fetch2R)
                 {
-                    int cnt = 0;
-                    if (lane == 0)
-                        cnt = traverse_sorted(P, o, dispersion * 2, S.leaves[j], kCLeaf);
-                    nl = __shfl_sync(0xffffffffu, cnt, 0);
-                    __syncwarp();
-                    ovf = nl < 0;
+                    redo |= 1u << j;     // the 2R fetch in the second round
+                    continue;
                 }
             }
             if (!ovf && fetch2R)
@@ -1649,6 +1687,8 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
                 qcol[qj] = out;
             }
             __syncwarp();
+        }
+        todo = redo;
         }
     }
 }
