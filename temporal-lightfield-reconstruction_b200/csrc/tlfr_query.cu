@@ -547,10 +547,9 @@ __device__ void flush_stats(const QStats& st, DevStats* ds)
 constexpr int kBlock = 128;
 // capacities of the full per-query path (statistics pass and heavy pass)
 constexpr int kStackCap = 96, kLeafCap = 256, kRsCap = 512, kSurfCap = 64;
-// capacities of the light pass, both in shared memory: the warp's traversal
-// stack (the union depth-first walk keeps at most one waiting sibling per level
-// of the hierarchy) and the leaf list per output sample
-constexpr int kLStack = 64, kLLeaf = 32;
+// capacities of the light pass: traversal stack and leaf list per output
+// sample, both in shared memory
+constexpr int kLStack = 16, kLLeaf = 32;
 
 // Per-thread column of a shared-memory array laid out [slot][thread]: a warp
 // whose lanes touch different slots still hits distinct banks.  The host build
@@ -606,109 +605,81 @@ TLFR_HD bool leaf_append(const QParams& P, const Query& o, const Column<float2>&
     return true;
 }
 
-// collectInputSamples2's traversal and leaf sort (RO.cpp:368-407) at radius R
-// for the warp's 32 output samples together.  The warp walks the union of the
-// nodes its lanes reach, depth first in the reference's order (push child0,
-// child1, pop the last); every stack entry carries the lanes for which all the
-// entry's ancestors intersected.  Children are stored as pairs, so a popped
-// entry loads both children once for the whole warp (one address for all
-// lanes) and each lane tests them against its own output sample.  Restricted
-// to the nodes one lane reaches, this order is that lane's own depth-first
-// order, so each lane's leaf column receives its leaves in the order the
-// reference's traversal finds them; FW::sort then orders them by key.  The
-// stack (wcap entries of node, lane mask) is shared by the warp.  All 32 lanes
-// call it; lanes with active false take no part.  Returns the lane's leaf
-// count, or -1 when its leaf column is full or the warp's stack is.
-__device__ int collect_packet(const QParams& P, int2* wstack, int wcap, const Column<float2>& leaves, int leaf_cap,
-                              const Query& o, float R, bool active)
+// collectInputSamples2's traversal and leaf sort (RO.cpp:368-407) for one output
+// sample at radius R: DFS in the reference's order (push child0, child1, pop the
+// last) into the leaf column, then FW::sort of the leaves by key.  Children are
+// stored as pairs, so a node that intersects has both children loaded and
+// tested together and only those that intersect are pushed (a leaf child waits
+// on the stack only behind an internal child1).  The loop has no early exit (an
+// overflow sets a flag), so a warp reconverges at the end of every step.
+// Returns the leaf count, or -1 when the stack or the leaf column is full.
+TLFR_HD int collect_pairs(const QParams& P, const Column<int>& stack, int stack_cap, const Column<float2>& leaves,
+                          int leaf_cap, const Query& o, float R)
 {
-    const int lane = threadIdx.x & 31;
     int nleaves = 0, sp = 0;
-    bool ok = true, wfull = false;
+    bool ok = true;
     {
         const QNode rn = load_node(P.nodes, P.root);
-        const bool h = active && node_intersect(rn, o, R);
-        const unsigned m = __ballot_sync(0xffffffffu, h);
-        if (rn.d.x < 0)
+        if (node_intersect(rn, o, R))
         {
-            if (h)
+            if (rn.d.x < 0)
                 ok = leaf_append(P, o, leaves, leaf_cap, nleaves, P.root, rn.d.z);
-        }
-        else if (m)
-        {
-            if (lane == 0)
-                wstack[0] = make_int2(rn.d.x, (int)m);
-            sp = 1;
+            else
+                stack[sp++] = rn.d.x;
         }
     }
-    __syncwarp();
-    // entries: x >= 0 the first child of a pair whose parent intersected; x < 0
-    // (~node) a leaf that intersected, waiting behind its internal sibling
-    while (sp > 0)
+    // stack entries: >= 0 the first child of an intersecting internal node;
+    // < 0 (~node) an intersecting leaf
+    while (sp > 0 && ok)
     {
-        const int2 e = wstack[--sp];
-        const bool in = ((unsigned)e.y >> lane) & 1u;
-        if (e.x < 0)
-        {
-            if (in && ok)
-                ok = leaf_append(P, o, leaves, leaf_cap, nleaves, ~e.x, P.nodes[~e.x].d.z);
-            continue;
-        }
-        const QNode n0 = load_node(P.nodes, e.x);
-        const QNode n1 = load_node(P.nodes, e.x + 1);
-        const bool h0 = in && node_intersect(n0, o, R);
-        const bool h1 = in && node_intersect(n1, o, R);
-        const unsigned m0 = __ballot_sync(0xffffffffu, h0);
-        const unsigned m1 = __ballot_sync(0xffffffffu, h1);
-        if (m1 && n1.d.x >= 0)
-        {
-            // child1's subtree comes first; child0 waits below it
-            const int np = m0 ? 2 : 1;
-            if (sp + np > wcap)
-            {
-                wfull = true;
-                break;
-            }
-            if (lane == 0)
-            {
-                if (m0)
-                    wstack[sp] = make_int2(n0.d.x >= 0 ? n0.d.x : ~e.x, (int)m0);
-                wstack[sp + np - 1] = make_int2(n1.d.x, (int)m1);
-            }
-            sp += np;
-        }
+        const int e = stack[--sp];
+        if (e < 0)
+            ok = leaf_append(P, o, leaves, leaf_cap, nleaves, ~e, P.nodes[~e].d.z);
         else
         {
-            if (h1 && ok)
-                ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e.x + 1, n1.d.z);
-            if (m0)
+            const QNode n0 = load_node(P.nodes, e);
+            const QNode n1 = load_node(P.nodes, e + 1);
+            const bool h0 = node_intersect(n0, o, R);
+            const bool h1 = node_intersect(n1, o, R);
+            if (h1 && n1.d.x >= 0)
             {
-                if (n0.d.x < 0)
-                {
-                    if (h0 && ok)
-                        ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e.x, n0.d.z);
-                }
-                else if (sp + 1 > wcap)
-                {
-                    wfull = true;
-                    break;
-                }
+                // child1's subtree comes first; child0 waits below it
+                if (sp + 2 > stack_cap)
+                    ok = false;
                 else
                 {
-                    if (lane == 0)
-                        wstack[sp] = make_int2(n0.d.x, (int)m0);
-                    sp++;
+                    if (h0)
+                        stack[sp++] = n0.d.x >= 0 ? n0.d.x : ~e;
+                    stack[sp++] = n1.d.x;
+                }
+            }
+            else
+            {
+                if (h1)
+                    ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e + 1, n1.d.z);
+                if (h0 && ok)
+                {
+                    if (n0.d.x < 0)
+                        ok = leaf_append(P, o, leaves, leaf_cap, nleaves, e, n0.d.z);
+                    else if (sp + 1 > stack_cap)
+                        ok = false;
+                    else
+                        stack[sp++] = n0.d.x;
                 }
             }
         }
-        __syncwarp();
     }
-    __syncwarp();
-    if (wfull || !ok)
+    if (!ok)
         return -1;
     LLeafSort ls{ leaves };
     fw_sort(ls, 0, nleaves);
     return nleaves;
+}
+
+// Light pass, part 1: each lane collects its own output sample's leaves at 1R.
+TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Column<float2>& leaves, const Query& o)
+{
+    return collect_pairs(P, stack, kLStack, leaves, kLLeaf, o, P.disp0);
 }
 
 // Light pass, part 2 (RO.cpp:94-99, 165-304 for the common case): the 1R scan
@@ -1045,10 +1016,10 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
               int* __restrict__ heavy_count)
 {
     __shared__ float2 sh_leaves[kLLeaf][kBlock];
-    __shared__ int2 sh_stack[kBlock / 32][kLStack];
+    __shared__ int sh_stack[kLStack][kBlock];
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
-    int2* wstack = sh_stack[threadIdx.x >> 5];
+    const Column<int> stack{ &sh_stack[0][threadIdx.x], kBlock };
     for (long long u = blockIdx.x; u < L.units; u += gridDim.x)
     {
         // each lane: traversal and leaf sort of its own output sample
@@ -1059,12 +1030,11 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
         const long long pix = valid ? (PROBE ? q / kProbe : q / P.M) : 0;
         const bool fast = !PROBE && valid && P.route_fast && P.route_fast[pix];
         if (valid)
+        {
             o = PROBE ? make_query(P, (int)(pix % P.W), (int)(pix / P.W), (int)((q % kProbe) * P.M / kProbe))
                       : query_of(P, q);
-        nl = collect_packet(P, wstack, kLStack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, kLLeaf, o,
-                            P.disp0, valid);
-        if (!valid)
-            nl = -2;
+            nl = light_collect(P, stack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, o);
+        }
         const unsigned fast_lanes = __ballot_sync(0xffffffffu, fast);
         __syncwarp();
         // the warp: the 1R scan of each lane's output sample in turn
