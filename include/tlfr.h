@@ -225,6 +225,15 @@ enum
 tlfr_status tlfr_synth_scene(int preset, int width, int height, int spp, unsigned long long seed,
                              float* records, float* coc_out);
 
+/* Reference image of a synthetic scene (the ground truth against which a
+ * reconstruction's PSNR is measured): per pixel the mean colour of the
+ * analytic scene over `samples` points spread over the pixel, the unit lens
+ * disk and the shutter [0, 1], computed on the current CUDA device; rgba
+ * receives width*height*4 floats (host memory).  No counterpart in the
+ * reference, whose ground-truth images came from its renderer.              */
+tlfr_status tlfr_synth_reference_image(int preset, int width, int height, int samples, unsigned long long seed,
+                                       float* rgba);
+
 /* ---- learned routing (no counterpart in the reference) --------------------
  * The router has no counterpart in the reference: a small network predicts, per pixel,
  * whether the fast path reproduces the plain method there; pixels above the

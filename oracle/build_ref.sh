@@ -92,8 +92,8 @@ compile "$OUT/obj/m128/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$SRC/rec
 compile "$OUT/obj/m64/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$OUT/gen_m64/reconstruction" & pids+=($!)
 # the seeded scene generator (the package's own host code, renamed), so that the
 # reference's CPU runs need no other library of this repository
-$CXX -std=c++17 -O2 -fPIC -ffp-contract=off -fno-fast-math -pthread -Dtlfr_synth_scene=ref_synth_scene \
-  -I"$HERE/../include" -c "$HERE/../temporal-lightfield-reconstruction_b200/csrc/synth_scene.cpp" \
+$CXX -std=c++17 -O2 -fPIC -ffp-contract=off -fno-fast-math -pthread -Dtlfr_synth_scene=ref_synth_scene -DTLFR_SYNTH_HOST_ONLY \
+  -I"$HERE/../include" -I"$HERE/../temporal-lightfield-reconstruction_b200/csrc" -c "$HERE/../temporal-lightfield-reconstruction_b200/csrc/synth_scene.cpp" \
   -o "$OUT/obj/ref_synth_scene.o" & pids+=($!)
 for p in "${pids[@]}"; do wait "$p"; done
 objs+=("$OUT/obj/ref_synth_scene.o")

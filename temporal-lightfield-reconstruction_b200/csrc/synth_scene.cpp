@@ -29,6 +29,7 @@
 // permutation.  All randomness comes from a counter-based hash of (seed, stream,
 // index), so the output does not depend on the thread count.
 #include "tlfr.h"
+#include "synth_model.h"
 
 #include <algorithm>
 #include <cmath>
@@ -40,52 +41,7 @@
 namespace
 {
 
-inline uint64_t mix64(uint64_t z)
-{
-    z += 0x9e3779b97f4a7c15ull;
-    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-    return z ^ (z >> 31);
-}
-
-inline uint64_t hash3(uint64_t a, uint64_t b, uint64_t c)
-{
-    return mix64(a ^ mix64(b ^ mix64(c)));
-}
-
-// uniform float in [0,1) from a hash
-inline float u01(uint64_t h) { return (float)((h >> 40) * (1.0 / 16777216.0)); }
-
-struct Card
-{
-    float w0, dw;
-    float cx, cy;       // pinhole centre at t=0, pixels
-    float hx, hy;       // half-size at depth w0, pixels
-    float dx, dy;       // screen motion over the shutter, pixels
-    int   disk;
-    float cell;         // value-noise lattice spacing, pixels at w0
-    uint64_t tex;       // texture seed
-    float bx0, by0, bx1, by1;   // sample-space bounding box (all t, all lens positions)
-};
-
-float value_noise(const Card& c, float a, float b, int ch)
-{
-    // lattice in card-local pixel units
-    float fx = (a * c.hx + c.hx) / c.cell;
-    float fy = (b * c.hy + c.hy) / c.cell;
-    float ix = std::floor(fx), iy = std::floor(fy);
-    float tx = fx - ix, ty = fy - iy;
-    tx = tx * tx * (3.0f - 2.0f * tx);
-    ty = ty * ty * (3.0f - 2.0f * ty);
-    auto v = [&](float i, float j) {
-        return u01(hash3(c.tex, (uint64_t)(int64_t)i * 2654435761ull + (uint64_t)ch, (uint64_t)(int64_t)j));
-    };
-    float v00 = v(ix, iy), v10 = v(ix + 1, iy), v01 = v(ix, iy + 1), v11 = v(ix + 1, iy + 1);
-    float r = (v00 * (1 - tx) + v10 * tx) * (1 - ty) + (v01 * (1 - tx) + v11 * tx) * ty;
-    return std::min(std::max(r, 0.0f), 1.0f);
-}
-
-float coc(float C0, float C1, float w) { return C0 / w + C1; }
+using namespace tlfr_synth;
 
 void card_bounds(Card& c, float C0, float C1)
 {
@@ -177,33 +133,6 @@ std::vector<Card> make_cards(const SceneDesc& d)
     return cards;
 }
 
-// Visible card and its local coordinates for one sample; returns the card index.
-int shade(const std::vector<Card>& cards, const std::vector<int>& cand, const SceneDesc& d,
-          float x, float y, float u, float v, float t, float* W_out, float* a_out, float* b_out)
-{
-    int best = -1;
-    float bestW = 3.0e38f, ba = 0, bb = 0;
-    for (int idx : cand)
-    {
-        const Card& c = cards[idx];
-        float W = c.w0 + t * c.dw;
-        if (!(W < bestW))
-            continue;
-        float r = coc(d.C0, d.C1, W);
-        float px = x - r * u, py = y - r * v;
-        float s = W / c.w0;
-        float lx = px * s - c.cx - t * c.dx;
-        float ly = py * s - c.cy - t * c.dy;
-        float a = lx / c.hx, b = ly / c.hy;
-        bool inside = c.disk ? (a * a + b * b <= 1.0f) : (std::fabs(a) <= 1.0f && std::fabs(b) <= 1.0f);
-        if (!inside)
-            continue;
-        best = idx; bestW = W; ba = a; bb = b;
-    }
-    *W_out = bestW; *a_out = ba; *b_out = bb;
-    return best;
-}
-
 // spp samples on an nx*ny stratification grid, nx >= ny (exact for powers of two)
 int grid_nx(int n) { int nx = 1, ny = 1; while (nx * ny < n) { if (nx <= ny) nx *= 2; else ny *= 2; } return nx; }
 int grid_ny(int n) { int nx = 1, ny = 1; while (nx * ny < n) { if (nx <= ny) nx *= 2; else ny *= 2; } return ny; }
@@ -261,7 +190,7 @@ void generate(const SceneDesc& d, float* out, int num_threads)
                 float t = ((float)perm_t[i] + r(4)) / spp;
                 if (t > 1.0f) t = 1.0f;
                 float Wv, a, b;
-                int ci = shade(cards, cand, d, x_s, y_s, u, v, t, &Wv, &a, &b);
+                int ci = shade(cards.data(), cand.data(), (int)cand.size(), d.C0, d.C1, x_s, y_s, u, v, t, &Wv, &a, &b);
                 if (ci < 0)
                 {   // cannot happen with the background card; keep the record valid
                     ci = 0; Wv = cards[0].w0; a = 0; b = 0;
@@ -294,31 +223,44 @@ void generate(const SceneDesc& d, float* out, int num_threads)
 
 } // namespace
 
-extern "C" tlfr_status tlfr_synth_scene(int preset, int width, int height, int spp, unsigned long long seed,
-                                        float* records, float* coc_out)
+namespace
 {
-    if (!records || width <= 0 || height <= 0 || spp <= 0 || spp > 256)
-        return TLFR_BAD_ARG;
-    SceneDesc d{};
+
+// Scene description of a preset (TLFR_SCENE_*); false for an unknown preset.
+bool preset_desc(int preset, int width, int height, int spp, unsigned long long seed, SceneDesc& d)
+{
+    d = SceneDesc{};
     d.W = width; d.H = height; d.spp = spp; d.seed = seed;
     switch (preset)
     {
     case TLFR_SCENE_PLANES:         // three fronto-parallel planes, defocus only
         d.mode = 0; d.C0 = -15.24f; d.C1 = 19.05f; d.bg_w = 12.0f; d.w_min = 2.0f; d.w_max = 12.0f;
-        break;
+        return true;
     case TLFR_SCENE_CARDS:          // 64 moving rectangles, defocus + motion
         d.mode = 1; d.C0 = -15.24f; d.C1 = 19.05f; d.num_rects = 64; d.num_disks = 0;
         d.w_min = 1.0f; d.w_max = 50.0f; d.side_min = 20.0f; d.side_max = 300.0f;
         d.motion_max = 40.0f; d.dw_frac = 0.1f; d.bg_w = 60.0f;
-        break;
+        return true;
     case TLFR_SCENE_CARDS_LARGE:    // 256 rectangles + 64 disks, strong blur, fast motion
         d.mode = 1; d.C0 = -30.0f; d.C1 = 40.0f; d.num_rects = 256; d.num_disks = 64;
         d.w_min = 0.5f; d.w_max = 100.0f; d.side_min = 20.0f; d.side_max = 300.0f;
         d.motion_max = 60.0f; d.dw_frac = 0.1f; d.bg_w = 120.0f;
-        break;
+        return true;
     default:
-        return TLFR_BAD_ARG;
+        return false;
     }
+}
+
+} // namespace
+
+extern "C" tlfr_status tlfr_synth_scene(int preset, int width, int height, int spp, unsigned long long seed,
+                                        float* records, float* coc_out)
+{
+    if (!records || width <= 0 || height <= 0 || spp <= 0 || spp > 256)
+        return TLFR_BAD_ARG;
+    SceneDesc d;
+    if (!preset_desc(preset, width, height, spp, seed, d))
+        return TLFR_BAD_ARG;
     unsigned hc = std::thread::hardware_concurrency();
     generate(d, records, hc ? (int)hc : 1);
     if (coc_out)
@@ -328,3 +270,38 @@ extern "C" tlfr_status tlfr_synth_scene(int preset, int width, int height, int s
     }
     return TLFR_OK;
 }
+
+#ifndef TLFR_SYNTH_HOST_ONLY
+extern "C" tlfr_status tlfr_synth_reference_image(int preset, int width, int height, int samples,
+                                                  unsigned long long seed, float* rgba)
+{
+    if (!rgba || width <= 0 || height <= 0 || samples <= 0 || samples > (1 << 16))
+        return TLFR_BAD_ARG;
+    SceneDesc d;
+    if (!preset_desc(preset, width, height, 1, seed, d))
+        return TLFR_BAD_ARG;
+    std::vector<Card> cards = make_cards(d);
+    // cards binned into 32x32-pixel tiles by their sample-space bounding boxes
+    // (as the generator does), as one list per tile
+    const int TS = 32;
+    const int tx = (d.W + TS - 1) / TS, ty = (d.H + TS - 1) / TS;
+    std::vector<std::vector<int>> bins((size_t)tx * ty);
+    for (int k = 0; k < (int)cards.size(); k++)
+    {
+        const Card& c = cards[k];
+        int x0 = std::max(0, (int)std::floor(c.bx0 / TS)), x1 = std::min(tx - 1, (int)std::floor(c.bx1 / TS));
+        int y0 = std::max(0, (int)std::floor(c.by0 / TS)), y1 = std::min(ty - 1, (int)std::floor(c.by1 / TS));
+        for (int j = y0; j <= y1; j++)
+            for (int i = x0; i <= x1; i++)
+                bins[(size_t)j * tx + i].push_back(k);
+    }
+    std::vector<int> start(1, 0), items;
+    for (auto& b : bins)
+    {
+        items.insert(items.end(), b.begin(), b.end());
+        start.push_back((int)items.size());
+    }
+    return (tlfr_status)tlfr_synth::integrate_image(cards.data(), (int)cards.size(), start.data(), items.data(), (int)items.size(),
+                                       tx, TS, d.C0, d.C1, d.W, d.H, samples, seed, rgba);
+}
+#endif

@@ -107,6 +107,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_query_samples_noalloc": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
         "tlfr_synth_scene": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_ulonglong, _FP, _FP]),
+        "tlfr_synth_reference_image": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                      ctypes.c_ulonglong, _FP]),
         "tlfr_route_features": (ctypes.c_int, [_VP, _VP]),
         "tlfr_route_labels": (ctypes.c_int, [_VP, ctypes.c_float, _VP, _VP]),
         "tlfr_router_create": (ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_uint, _FP, _FP, ctypes.POINTER(_VP)]),
@@ -157,6 +159,16 @@ def synth_scene(preset: int, width: int, height: int, spp: int, seed: int = 1):
     coc = np.zeros(2, np.float32)
     _check(lib.tlfr_synth_scene(preset, width, height, spp, seed, _f32p(rec), _f32p(coc)))
     return rec, (float(coc[0]), float(coc[1]))
+
+
+def synth_reference_image(preset: int, width: int, height: int, samples: int = 1024, seed: int = 1) -> np.ndarray:
+    """Ground-truth RGBA image [H, W, 4] of the seeded scene: the mean colour
+    over `samples` points per pixel spread over the pixel, the unit lens disk
+    and the shutter (computed on the current CUDA device)."""
+    lib = load_library()
+    img = np.empty((height, width, 4), np.float32)
+    _check(lib.tlfr_synth_reference_image(preset, width, height, samples, seed, _f32p(img)))
+    return img
 
 
 class UVTSampleBuffer:

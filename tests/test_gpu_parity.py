@@ -192,3 +192,26 @@ def test_gpu_all_samples_discarded_reports_empty():
     with pytest.raises(tlfr.TlfrError) as e:
         gpu_recon(rec, coc)
     assert e.value.status == 9   # TLFR_EMPTY
+
+
+FULL_FRAMES = [
+    # the 256x256, 16 spp three-plane frame with 64 output samples per pixel
+    ("planes_256x256x16_m64", tlfr.SCENE_PLANES, 256, 256, 16, 3, {"output_spp": 64}),
+    # the 962x543, 4 spp 64-card frame (defocus and motion), blurred and as the t=1 pinhole image
+    ("cards_962x543x4", tlfr.SCENE_CARDS, 962, 543, 4, 4, {}),
+    ("cards_962x543x4_pinhole", tlfr.SCENE_CARDS, 962, 543, 4, 4, {"uvt": (0.0, 0.0, 1.0)}),
+]
+
+
+@pytest.mark.parametrize("name,preset,W,H,spp,seed,p", FULL_FRAMES, ids=[s[0] for s in FULL_FRAMES])
+def test_gpu_full_frame_matches_oracle(name, preset, W, H, spp, seed, p):
+    """Whole frames of the stated workload sizes, every pixel against the oracle."""
+    import os
+    rec, coc = tlfr.synth_scene(preset, W, H, spp, seed)
+    kw = dict(uvt=p.get("uvt"), output_spp=p.get("output_spp", 0))
+    g = gpu_recon(rec, coc, **kw)
+    img = g.reconstructDofMotion()
+    o = CpuRecon("orc", rec, coc, nthreads=os.cpu_count() or 8, **kw)
+    ref = o.reconstruct()
+    assert rel_err(img, ref).max() <= RTOL
+    assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
