@@ -63,9 +63,12 @@ def parse():
     ap.add_argument("--width", type=int, default=W)
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
-    ap.add_argument("--route-frames", type=int, default=2, help="router training frames (0: no routed run)")
+    ap.add_argument("--route-frames", type=int, default=32, help="router training frames, seeds 100.. (0: no routed run)")
+    ap.add_argument("--route-eval", type=int, default=8, help="held-out evaluation frames, seeds 200..")
     ap.add_argument("--route-steps", type=int, default=600)
     ap.add_argument("--route-threshold", type=float, default=0.8)
+    ap.add_argument("--route-tol", type=float, default=0.005, help="label tolerance (max channel difference)")
+    ap.add_argument("--gt-samples", type=int, default=1024, help="ground-truth samples per pixel")
     ap.add_argument("--batch-frames", type=int, default=48, help="uneven-buffer batch size (0: no batch run)")
     ap.add_argument("--batch-scale", type=int, default=4, help="linear downscale of the batch's resolutions")
     ap.add_argument("--profile-frame", action="store_true",
@@ -228,12 +231,21 @@ def cpu_baseline_sample(rec, coc, rows, threads, gpu_img=None):
     return out
 
 
+def psnr(img, ref):
+    """PSNR in dB of the RGB channels of img against ref (peak 1)."""
+    import numpy as np
+    mse = float(np.mean((img[..., :3].astype(np.float64) - ref[..., :3].astype(np.float64)) ** 2))
+    return 10 * float(np.log10(1.0 / mse)) if mse > 0 else float("inf")
+
+
 def train_router(args, device, W, H, S):
-    """Learned router trained on plain-method labels of held-out frames (seeds 100+), untimed."""
+    """The learned router trained on plain-method labels of args.route_frames
+    frames of the strong-blur scene (seeds 100, 101, ...), untimed."""
     import numpy as np
     import torch
     import tlfr
     feats, labels = [], []
+    t0 = time.perf_counter()
     for seed in range(100, 100 + args.route_frames):
         rec, coc = tlfr.synth_scene(PRESET, W, H, S, seed)
         d = torch.from_numpy(rec).cuda()
@@ -242,23 +254,95 @@ def train_router(args, device, W, H, S):
         lab = torch.empty(H * W, dtype=torch.float32, device="cuda")
         img = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
         g.route_features(f.data_ptr())
-        g.route_labels(lab.data_ptr(), img.data_ptr(), 0.01)
+        g.route_labels(lab.data_ptr(), img.data_ptr(), args.route_tol)
         feats.append(f)
         labels.append(lab)
         g.close()
         del d
+    label_s = time.perf_counter() - t0
     F = torch.cat(feats)
     L = torch.cat(labels)
-    fh = F.cpu().numpy()
+    del feats, labels
+    fh = F[::97].cpu().numpy()
     router = tlfr.Router(device, seed=3, mean=fh.mean(0), inv_std=1.0 / np.maximum(fh.std(0), 1e-6))
     n = F.shape[0]
-    loss0 = router.gradient(F.data_ptr(), L.data_ptr(), n)[1]
+    loss0 = router.gradient(F.data_ptr(), L.data_ptr(), min(n, 1 << 20))[1]
     t0 = time.perf_counter()
     loss = router.train(F.data_ptr(), L.data_ptr(), n, steps=args.route_steps, batch=8192, lr=3e-3)
     info = {"frames": args.route_frames, "seeds": [100, 100 + args.route_frames - 1], "pixels": n,
-            "label_mean": float(L.mean().item()), "label_tolerance": 0.01, "steps": args.route_steps,
-            "loss_initial": loss0, "loss_final": loss, "train_s": time.perf_counter() - t0}
+            "label_mean": float(L.mean().item()), "label_tolerance": args.route_tol, "steps": args.route_steps,
+            "loss_initial": loss0, "loss_final": loss, "train_s": time.perf_counter() - t0, "labels_s": label_s}
+    del F, L
+    torch.cuda.empty_cache()
     return router, info
+
+
+def routing_eval(args, device, router, W, H, S):
+    """The router on held-out frames (seeds 200, 201, ...): per seed the plain
+    method, the routed form and every pixel on the fast path (no network), each
+    timed over full steps (hierarchy build + reconstruction, CUDA events), and
+    each image's PSNR against the scene's ground truth (tlfr.synth_reference_image)."""
+    import numpy as np
+    import torch
+    import tlfr
+    stream = torch.cuda.current_stream()
+    rows = []
+    for seed in range(200, 200 + args.route_eval):
+        rec, coc = tlfr.synth_scene(PRESET, W, H, S, seed)
+        d = torch.from_numpy(rec).cuda()
+        g = tlfr.TreeGather(None, tlfr.CameraParams(device=device), stream=stream.cuda_stream,
+                            device_records=(d.data_ptr(), (W, H, S), coc))
+        out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+
+        def timed(router_, thr, k=2):
+            g.set_routing(router_, thr)
+            g.rebuild(d.data_ptr())
+            g.reconstruct_to_device(out.data_ptr())
+            ms = []
+            for _ in range(k):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                g.rebuild(d.data_ptr())
+                g.reconstruct_to_device(out.data_ptr())
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            return statistics.median(ms), out.cpu().numpy()
+
+        ms_plain, plain = timed(None, 0.8)
+        ms_routed, routed = timed(router, args.route_threshold)
+        ms_all, allfast = timed(router, 0.0)
+        feats = torch.empty((H * W, 8), dtype=torch.float32, device="cuda")
+        prob = torch.empty(H * W, dtype=torch.float32, device="cuda")
+        g.route_features(feats.data_ptr())
+        router.predict(feats.data_ptr(), W * H, prob.data_ptr())
+        frac = float((prob > args.route_threshold).float().mean().item())
+        g.set_routing(None)
+        g.close()
+        del d
+        gt = tlfr.synth_reference_image(PRESET, W, H, args.gt_samples, seed)
+        p_plain, p_routed, p_all = psnr(plain, gt), psnr(routed, gt), psnr(allfast, gt)
+        rows.append({
+            "seed": seed, "plain_ms": ms_plain, "routed_ms": ms_routed, "all_fast_ms": ms_all,
+            "speedup": ms_plain / ms_routed, "fast_pixel_fraction": frac,
+            "psnr_plain_db": p_plain, "psnr_routed_db": p_routed, "psnr_all_fast_db": p_all,
+            "psnr_loss_db": p_plain - p_routed, "psnr_loss_all_fast_db": p_plain - p_all,
+            "max_abs_err_vs_plain": float(np.abs(routed[..., :3] - plain[..., :3]).max()),
+            "psnr_routed_vs_plain_db": psnr(routed, plain),
+        })
+    med = lambda k: statistics.median(r[k] for r in rows)
+    return {
+        "seeds": [r["seed"] for r in rows], "per_seed": rows,
+        "speedup_median": med("speedup"), "speedup_all_fast_median": statistics.median(
+            r["plain_ms"] / r["all_fast_ms"] for r in rows),
+        "psnr_loss_db_max": max(r["psnr_loss_db"] for r in rows), "psnr_loss_db_median": med("psnr_loss_db"),
+        "psnr_loss_all_fast_db_median": med("psnr_loss_all_fast_db"),
+        "fast_pixel_fraction_median": med("fast_pixel_fraction"),
+        "value": (W * H / (med("routed_ms") / 1e3)) / 1e6, "unit": "Mpix/s",
+        "threshold": args.route_threshold, "gt_samples_per_pixel": args.gt_samples,
+        "timing": "median of 2 full steps (hierarchy build + reconstruction) per seed after one warm-up, CUDA events",
+    }
 
 
 def max_over_ranks(value, dist, device="cuda"):
@@ -471,44 +555,14 @@ def main():
     value = (world * Wd * Hd * args.steps / (total_ms / 1e3)) / 1e6
     plain_host = out.cpu().numpy()          # the timed frame, for the parity check of cpu_baseline
 
-    # learned routing: the same frame and timing with the router on, against the plain image
+    # learned routing: trained on route_frames plain-method frames (seeds 100+),
+    # evaluated on route_eval held-out frames (seeds 200+) against ground truth
     routed = None
+    router = None
     if args.route_frames > 0:
-        plain_img = out.clone()
         router, rinfo = train_router(args, local_rank, Wd, Hd, S)
-        tg.set_routing(router, args.route_threshold)
-        for _ in range(max(3, args.warmup)):
-            step()
-        torch.cuda.synchronize()
-        barrier()
-        r0 = torch.cuda.Event(enable_timing=True)
-        r1 = torch.cuda.Event(enable_timing=True)
-        r0.record(stream)
-        for _ in range(args.steps):
-            step()
-        r1.record(stream)
-        torch.cuda.synchronize()
-        r_ms = r0.elapsed_time(r1)
-        r_ms = max_over_ranks(r_ms, dist)
-        rs = tg.stats()
-        import numpy as np
-        a = out[..., :3].double()
-        b = plain_img[..., :3].double()
-        mse = float(((a - b) ** 2).mean().item())
-        prob = torch.empty(Wd * Hd, dtype=torch.float32, device="cuda")
-        feats = torch.empty((Hd * Wd, 8), dtype=torch.float32, device="cuda")
-        tg.route_features(feats.data_ptr())
-        router.predict(feats.data_ptr(), Wd * Hd, prob.data_ptr())
-        routed = {
-            "value": (world * Wd * Hd * args.steps / (r_ms / 1e3)) / 1e6, "unit": "Mpix/s",
-            "ms_per_step": r_ms / args.steps, "speedup_vs_plain": total_ms / r_ms,
-            "psnr_vs_plain_db": (10 * float(np.log10(1.0 / mse))) if mse > 0 else None,
-            "max_abs_err_vs_plain": float((a - b).abs().max().item()),
-            "fast_pixel_fraction": float((prob > args.route_threshold).float().mean().item()),
-            "threshold": args.route_threshold, "heavy_queries": rs.num_heavy_queries,
-            "light_pass_ms": rs.light_ms, "heavy_pass_ms": rs.heavy_ms, "train": rinfo,
-        }
-        tg.set_routing(None)
+        routed = routing_eval(args, local_rank, router, Wd, Hd, S)
+        routed["train"] = rinfo
 
     # uneven-buffer batch (one CUDA graph), learned routing on
     batch = None
