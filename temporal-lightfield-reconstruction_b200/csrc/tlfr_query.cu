@@ -614,7 +614,7 @@ TLFR_HD bool leaf_append(const QParams& P, const Query& o, const Column<float2>&
 // overflow sets a flag), so a warp reconverges at the end of every step.
 // Returns the leaf count, or -1 when the stack or the leaf column is full.
 TLFR_HD int collect_pairs(const QParams& P, const Column<int>& stack, int stack_cap, const Column<float2>& leaves,
-                          int leaf_cap, const Query& o, float R, bool sort = true)
+                          int leaf_cap, const Query& o, float R)
 {
     int nleaves = 0, sp = 0;
     bool ok = true;
@@ -671,46 +671,15 @@ TLFR_HD int collect_pairs(const QParams& P, const Column<int>& stack, int stack_
     }
     if (!ok)
         return -1;
-    if (sort)
-    {
-        LLeafSort ls{ leaves };
-        fw_sort(ls, 0, nleaves);
-    }
+    LLeafSort ls{ leaves };
+    fw_sort(ls, 0, nleaves);
     return nleaves;
 }
 
-// Light pass, part 1: each lane collects its own output sample's leaves at 1R
-// (unsorted for the router's single-surface fast path, which sums in any order).
-TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Column<float2>& leaves, const Query& o,
-                          bool sort)
+// Light pass, part 1: each lane collects its own output sample's leaves at 1R.
+TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Column<float2>& leaves, const Query& o)
 {
-    return collect_pairs(P, stack, kLStack, leaves, kLLeaf, o, P.disp0, sort);
-}
-
-// Reprojection of sample i to the query's (u,v,t) and its squared distance
-// (RO.cpp:436-454); the same operations as collect().
-__device__ __forceinline__ float reproject(const QParams& P, int i, const Query& o, float& x, float& y)
-{
-    float4 sp4, sm;
-    load_sample(P.s_rec, i, sp4, sm);
-    if (sm.x != 0.0f || sm.y != 0.0f || sm.z != 0.0f)
-    {
-        const float dt = o.t - sp4.w;
-        const float Px = sp4.x * sp4.z + sm.x * dt;
-        const float Py = sp4.y * sp4.z + sm.y * dt;
-        const float Pw = (1.0f * sp4.z) + sm.z * dt;
-        const float cr = rcp(Pw);
-        const float coc = P.c0 / Pw + P.c1;
-        x = Px * cr + o.u * coc;
-        y = Py * cr + o.v * coc;
-    }
-    else
-    {
-        x = sp4.x + o.u * sm.w;
-        y = sp4.y + o.v * sm.w;
-    }
-    const float dx = x - o.x, dy = y - o.y;
-    return dx * dx + dy * dy;
+    return collect_pairs(P, stack, kLStack, leaves, kLLeaf, o, P.disp0);
 }
 
 // sameSurface's sixteen plane values of one node for one output sample: each
@@ -764,10 +733,14 @@ TLFR_HD bool same_surface_vals(const SurfVals& a, const SurfVals& b)
 // against every leaf since the surface opened (RO.cpp:465-470), lanes over
 // those leaves; when one fails the scan stops there.  All lanes call it with
 // the same arguments and get the same result: 0 with the colour in out, 1
-// when the output sample needs the 2R fetch.  *multi is set when a second
-// surface opened (the router's coarse pass counts it).
+// when the output sample needs the 2R fetch.
+// first_surface (the learned router's fast path for pixels it marks as holding
+// a single apparent surface; no reference counterpart): when a second surface
+// opens, the first one is taken even if its samples do not cover all four
+// quadrants, where the reference would refetch at 2R.  Output samples with
+// nothing within 1R still take the full path.
 __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, int nleaves, const Query& o,
-                               float4& out, bool* multi = nullptr)
+                               float4& out, bool first_surface = false)
 {
     const int lane = threadIdx.x & 31;
     const float R = P.disp0;
@@ -901,9 +874,7 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
                         const bool sj = (lane >= lidx0 && lane < kseg) ? same_surface_vals(cur, my_sv) : true;
                         if (!__all_sync(0xffffffffu, sj))   // a second surface opens: the first one is final
                         {
-                            result = quad == 0xF ? 0 : 1;
-                            if (multi)
-                                *multi = true;
+                            result = (quad == 0xF || first_surface) ? 0 : 1;
                             break;
                         }
                     }
@@ -943,106 +914,6 @@ __device__ int light_scan_warp(const QParams& P, const Column<float2>& leaves, i
     acc.x *= oow; acc.y *= oow; acc.z *= oow; acc.w *= oow;
     if (acc.w == 0)
         acc = P.s_col[nearest];
-    if (P.lens_filter == 1)
-    {
-        float g = gaussian(o.u, 0.5f, 0) * gaussian(o.v, 0.5f, 0);
-        acc.x *= g; acc.y *= g; acc.z *= g; acc.w *= g;
-    }
-    if (P.time_filter == 1)
-    {
-        float g = gaussian(o.t, 0.25f, 0.5f);
-        acc.x *= g; acc.y *= g; acc.z *= g; acc.w *= g;
-    }
-    out = acc;
-    return 0;
-}
-
-// The learned router's single-surface fast path (no reference counterpart),
-// for output samples of pixels the router marks as holding one apparent
-// surface: every sample within R of the output sample is taken as one
-// surface, so the leaves need no sort, and there are no sameSurface tests and
-// no quadrant bookkeeping; the tent filter (RO.cpp:274-294) is summed per lane
-// and then across the lanes, and the nearest sample is kept for the fallback
-// when no weight is positive (RO.cpp:318-348).  Where the plain method's 1R
-// fetch holds a single surface this is its result up to the order of the sum.
-// All lanes call it with the same arguments and get the same result: 0 with
-// the colour in out, 1 when nothing lies within R (the full path takes it).
-__device__ int light_scan_fast(const QParams& P, const Column<float2>& leaves, int nleaves, const Query& o,
-                               float4& out)
-{
-    const int lane = threadIdx.x & 31;
-    const float R = P.disp0;
-    const float R2 = R * R;
-    int my_s0 = 0, my_n = 0;
-    if (lane < nleaves)
-    {
-        const int4 d = P.nodes[leaf_node(leaves, lane)].d;
-        my_s0 = d.z;
-        my_n = d.w - d.z;
-    }
-    int my_f = my_n;
-    for (int off = 1; off < 32; off <<= 1)
-    {
-        const int v = __shfl_up_sync(0xffffffffu, my_f, off);
-        if (lane >= off)
-            my_f += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, my_f, 31);
-    my_f -= my_n;
-    float4 acc = make_float4(0, 0, 0, 0);
-    float best = __int_as_float(0x7f800000);
-    int best_i = -1;
-    bool any = false;
-    for (int base = 0; base < total; base += 32)
-    {
-        const bool starts_in = lane < nleaves && my_f > base && my_f < base + 32;
-        const unsigned starts = __reduce_or_sync(0xffffffffu, starts_in ? 1u << (my_f - base) : 0u);
-        const int k = __popc(__ballot_sync(0xffffffffu, lane < nleaves && my_f <= base)) - 1 +
-                      __popc(starts & ((2u << lane) - 1u));
-        const int i = __shfl_sync(0xffffffffu, my_s0, k & 31) + (base + lane - __shfl_sync(0xffffffffu, my_f, k & 31));
-        if (base + lane < total)
-        {
-            float x, y;
-            const float d2 = reproject(P, i, o, x, y);
-            if (d2 <= R2)
-            {
-                any = true;
-                const float dist = sqrtf(d2);
-                const float weight = 1 - dist / R;
-                if (weight > 0)
-                {
-                    const float4 c = P.s_col[i];
-                    acc.x += c.x * weight; acc.y += c.y * weight; acc.z += c.z * weight; acc.w += c.w * weight;
-                }
-                if (dist < best)
-                {
-                    best = dist;
-                    best_i = i;
-                }
-            }
-        }
-    }
-    if (!__any_sync(0xffffffffu, any))
-        return 1;
-    for (int off = 16; off > 0; off >>= 1)
-    {
-        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
-        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
-        acc.z += __shfl_xor_sync(0xffffffffu, acc.z, off);
-        acc.w += __shfl_xor_sync(0xffffffffu, acc.w, off);
-    }
-    if (acc.w == 0)
-    {
-        // every accepted sample lies at distance R: the nearest one's colour
-        const unsigned mb = __reduce_min_sync(0xffffffffu, __float_as_uint(best));
-        const int src = __ffs(__ballot_sync(0xffffffffu, __float_as_uint(best) == mb)) - 1;
-        acc = P.s_col[__shfl_sync(0xffffffffu, best_i, src)];
-    }
-    else
-    {
-        const float oow = rcp(acc.w);
-        acc.x *= oow; acc.y *= oow; acc.z *= oow; acc.w *= oow;
-    }
     if (P.lens_filter == 1)
     {
         float g = gaussian(o.u, 0.5f, 0) * gaussian(o.v, 0.5f, 0);
@@ -1139,10 +1010,7 @@ __device__ __forceinline__ bool light_query_id(const QParams& P, const LightMap&
     return x < P.W && y < P.H;
 }
 
-// ROUTED: the learned router's flags are read (P.route_fast) and flagged
-// pixels take the single-surface fast path; the plain method is the instance
-// without it.
-template <bool PROBE, bool ROUTED>
+template <bool PROBE>
 __global__ void __launch_bounds__(kBlock, kLightBlocksPerSM)
 k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
               int* __restrict__ heavy_count)
@@ -1160,18 +1028,17 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
         Query o{};
         int nl = -2;
         const long long pix = valid ? (PROBE ? q / kProbe : q / P.M) : 0;
-        const bool fast = ROUTED && !PROBE && valid && P.route_fast[pix];
+        const bool fast = !PROBE && valid && P.route_fast && P.route_fast[pix];
         if (valid)
         {
             o = PROBE ? make_query(P, (int)(pix % P.W), (int)(pix / P.W), (int)((q % kProbe) * P.M / kProbe))
                       : query_of(P, q);
-            nl = light_collect(P, stack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, o, !fast);
+            nl = light_collect(P, stack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, o);
         }
         const unsigned fast_lanes = __ballot_sync(0xffffffffu, fast);
         __syncwarp();
         // the warp: the 1R scan of each lane's output sample in turn
         int code = 2;
-        bool multi = false;
         float4 col = make_float4(0, 0, 0, 0);
         for (int j = 0; j < 32; j++)
         {
@@ -1186,22 +1053,18 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
             oj.t = __shfl_sync(0xffffffffu, o.t, j);
             float4 c;
             const Column<float2> lj{ &sh_leaves[0][wbase + j], kBlock };
-            bool mj = false;
-            const int r = (ROUTED && ((fast_lanes >> j) & 1u)) ? light_scan_fast(P, lj, nlj, oj, c)
-                                                               : light_scan_warp(P, lj, nlj, oj, c, &mj);
+            const int r = light_scan_warp(P, lj, nlj, oj, c, (fast_lanes >> j) & 1u);
             if (lane == j)
             {
                 code = r;
                 col = c;
-                multi = mj;
             }
         }
         __syncwarp();
         if (PROBE)
         {
-            // heavy_count is the per-pixel count here: probed output samples
-            // that see a second surface or need the full path
-            if (valid && (code != 0 || multi))
+            // heavy_count is the per-pixel count here
+            if (valid && code != 0)
                 atomicAdd(&heavy_count[pix], 1);
             continue;
         }
@@ -1261,6 +1124,32 @@ struct CoopScratch
 };
 
 __device__ __forceinline__ unsigned lanes_below(int lane) { return (1u << lane) - 1u; }
+
+// Reprojection of sample i to the query's (u,v,t) and its squared distance
+// (RO.cpp:436-454); the same operations as collect().
+__device__ __forceinline__ float reproject(const QParams& P, int i, const Query& o, float& x, float& y)
+{
+    float4 sp4, sm;
+    load_sample(P.s_rec, i, sp4, sm);
+    if (sm.x != 0.0f || sm.y != 0.0f || sm.z != 0.0f)
+    {
+        const float dt = o.t - sp4.w;
+        const float Px = sp4.x * sp4.z + sm.x * dt;
+        const float Py = sp4.y * sp4.z + sm.y * dt;
+        const float Pw = (1.0f * sp4.z) + sm.z * dt;
+        const float cr = rcp(Pw);
+        const float coc = P.c0 / Pw + P.c1;
+        x = Px * cr + o.u * coc;
+        y = Py * cr + o.v * coc;
+    }
+    else
+    {
+        x = sp4.x + o.u * sm.w;
+        y = sp4.y + o.v * sm.w;
+    }
+    const float dx = x - o.x, dy = y - o.y;
+    return dx * dx + dy * dy;
+}
 
 // DFS traversal into leaves[] with leaf keys (RO.cpp:368-395) and FW::sort of
 // the leaves (RO.cpp:407).  Returns the leaf count or -1 on overflow.
@@ -1919,15 +1808,6 @@ QParams make_params(const Ctx& c)
 
 int coop_blocks(const Ctx& c) { return c.num_sms * kCoopBlocksPerSM; }
 
-// The light pass launched as its plain or routed instance (router flags set).
-#define LIGHT_LAUNCH(c, P, grid, block, s, ...)                                                   \
-    do {                                                                                          \
-        if ((P).route_fast)                                                                       \
-            TLFR_LAUNCH(c, (k_query_light<false, true>), grid, block, s, __VA_ARGS__);           \
-        else                                                                                      \
-            TLFR_LAUNCH(c, (k_query_light<false, false>), grid, block, s, __VA_ARGS__);          \
-    } while (0)
-
 // overflow pass capacities
 constexpr int kOvStack = 512, kOvLeaf = 16384, kOvRs = 65536, kOvSurf = 4096;
 constexpr int kOvSlots = 4096;
@@ -1972,7 +1852,7 @@ tlfr_status route_probe(Ctx& c, int* d_counts)
     CKQ(cudaMemsetAsync(d_counts, 0, sizeof(int) * npix, s));
     const LightMap L = light_map(c, nq);
     const int blocks = (int)std::min<long long>(L.units, (long long)c.num_sms * 64);
-    TLFR_LAUNCH(c, (k_query_light<true, false>), blocks, kBlock, s, P, L, nq, nullptr, nullptr, d_counts);
+    TLFR_LAUNCH(c, k_query_light<true>, blocks, kBlock, s, P, L, nq, nullptr, nullptr, d_counts);
     CKQ(cudaGetLastError());
     return TLFR_OK;
 }
@@ -2062,7 +1942,7 @@ tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_bloc
         c.launches++;
         P.route_fast = c.route_fast;
     }
-    LIGHT_LAUNCH(c, P, light_blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
+    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
                 counters + 2);
     TLFR_LAUNCH(c, k_query_coop, coop_blocks(c), kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol, c.ovf_queue,
                 counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(coop_scratch));
@@ -2096,7 +1976,7 @@ tlfr_status light_trial(Ctx& c, cudaStream_t s, int light_blocks, float* ms)
     CKQ(cudaEventCreate(&e1));
     CKQ(cudaMemsetAsync(counters, 0, 8 * sizeof(int), s));
     CKQ(cudaEventRecord(e0, s));
-    LIGHT_LAUNCH(c, P, light_blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
+    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
                 counters + 2);
     CKQ(cudaEventRecord(e1, s));
     CKQ(cudaEventSynchronize(e1));
@@ -2184,7 +2064,7 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
             c.coop_scratch_bytes = coop_scratch_bytes(c.num_sms);
             CKQ(cudaMalloc(&c.coop_scratch, c.coop_scratch_bytes));
         }
-        LIGHT_LAUNCH(c, P, light_default_blocks(c), kBlock, s, P, light_map(c), nq, c.qcol,
+        TLFR_LAUNCH(c, k_query_light<false>, light_default_blocks(c), kBlock, s, P, light_map(c), nq, c.qcol,
                     c.heavy_queue, counters + 2);
         CKQ(cudaEventRecord(c.evq1, s));
         TLFR_LAUNCH(c, k_query_coop, coop_blocks(c), kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol,

@@ -150,30 +150,3 @@ def _always_fast(router):
         _ALWAYS["r"] = r
     return _ALWAYS["r"]
 
-
-@pytest.mark.gpu
-def test_fast_path_equals_plain_on_single_surface_pixels():
-    """The single-surface fast path takes every sample within 1R as one surface.
-    Where all of a pixel's output samples have one surface in the plain method's
-    1R fetch (no 2R refetch), the fast pixel is the plain pixel up to the order of
-    the tent filter's sum."""
-    torch = _torch()
-    W, H, S = 160, 96, 8
-    rec, coc = tlfr.synth_scene(tlfr.SCENE_CARDS_LARGE, W, H, S, 61)
-    g = tlfr.TreeGather(tlfr.UVTSampleBuffer(records=rec, coc=coc))
-    plain = g.reconstructDofMotion()
-    g.set_routing(_always_fast(None), 0.5)
-    fast = g.reconstructDofMotion()
-    g.set_routing(None)
-    rng = np.random.default_rng(62)
-    checked = 0
-    for _ in range(60):
-        x, y = int(rng.integers(0, W)), int(rng.integers(0, H))
-        q = np.array([[x, y, i] for i in range(128)], np.int32)
-        _rgba, tr = g.trace_queries(q, stride=4096)
-        if np.all(tr[:, 0] == 0) and np.all(tr[:, 1] == 1):
-            checked += 1
-            rel = np.abs(fast[y, x] - plain[y, x]) / np.maximum(np.abs(plain[y, x]), 1e-6)
-            assert rel.max() <= 1e-5, (x, y, fast[y, x], plain[y, x])
-    print(f"single-surface pixels checked: {checked}")
-    assert checked >= 10
