@@ -67,7 +67,10 @@ def parse():
     ap.add_argument("--route-eval", type=int, default=8, help="held-out evaluation frames, seeds 200..")
     ap.add_argument("--route-steps", type=int, default=600)
     ap.add_argument("--route-threshold", type=float, default=0.8)
-    ap.add_argument("--route-tol", type=float, default=0.005, help="label tolerance (max channel difference)")
+    ap.add_argument("--route-labels", default="gt", choices=["gt", "plain"],
+                    help="router labels against the scene's ground truth or the plain image")
+    ap.add_argument("--route-tol", type=float, default=2e-5,
+                    help="label tolerance: squared RGB error above the plain pixel's (gt) or channel difference")
     ap.add_argument("--gt-samples", type=int, default=1024, help="ground-truth samples per pixel")
     ap.add_argument("--batch-frames", type=int, default=48, help="uneven-buffer batch size (0: no batch run)")
     ap.add_argument("--batch-scale", type=int, default=4, help="linear downscale of the batch's resolutions")
@@ -254,7 +257,12 @@ def train_router(args, device, W, H, S):
         lab = torch.empty(H * W, dtype=torch.float32, device="cuda")
         img = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
         g.route_features(f.data_ptr())
-        g.route_labels(lab.data_ptr(), img.data_ptr(), args.route_tol)
+        if args.route_labels == "gt":
+            gt = torch.from_numpy(tlfr.synth_reference_image(PRESET, W, H, args.gt_samples, seed)).cuda()
+            g.route_labels(lab.data_ptr(), img.data_ptr(), args.route_tol, d_ref=gt.data_ptr())
+            del gt
+        else:
+            g.route_labels(lab.data_ptr(), img.data_ptr(), args.route_tol)
         feats.append(f)
         labels.append(lab)
         g.close()
@@ -270,7 +278,10 @@ def train_router(args, device, W, H, S):
     t0 = time.perf_counter()
     loss = router.train(F.data_ptr(), L.data_ptr(), n, steps=args.route_steps, batch=8192, lr=3e-3)
     info = {"frames": args.route_frames, "seeds": [100, 100 + args.route_frames - 1], "pixels": n,
-            "label_mean": float(L.mean().item()), "label_tolerance": args.route_tol, "steps": args.route_steps,
+            "label_mean": float(L.mean().item()), "label_tolerance": args.route_tol, "label_reference":
+            "ground truth (fast pixel's squared RGB error at most tol above the plain pixel's)"
+            if args.route_labels == "gt" else "plain method (max channel difference at most tol)",
+            "steps": args.route_steps,
             "loss_initial": loss0, "loss_final": loss, "train_s": time.perf_counter() - t0, "labels_s": label_s}
     del F, L
     torch.cuda.empty_cache()

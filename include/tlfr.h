@@ -252,6 +252,10 @@ tlfr_status tlfr_route_features(tlfr_ctx* ctx, float* d_feats);
  * and the per-pixel labels (device, width*height floats): 1 where the fast
  * path reproduces the plain pixel within tol on every channel, 0 elsewhere. */
 tlfr_status tlfr_route_labels(tlfr_ctx* ctx, float tol, float* d_labels, float* d_rgba);
+/* The same with the scene's ground truth d_ref (device RGBA, W*H*4 floats): a
+ * pixel's label is 1 where the fast path's squared RGB error against d_ref is
+ * at most tol above the plain method's.                                      */
+tlfr_status tlfr_route_labels_ref(tlfr_ctx* ctx, const float* d_ref, float tol, float* d_labels, float* d_rgba);
 /* New 8-64-64-1 network on a device, He-initialised from seed; mean8/inv_std8
  * (host, 8 floats each, may be null) standardise the features. */
 tlfr_status tlfr_router_create(int device, void* stream, unsigned seed, const float* mean8, const float* inv_std8,

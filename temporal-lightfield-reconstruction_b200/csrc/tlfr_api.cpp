@@ -959,6 +959,11 @@ tlfr_status tlfr_route_features(tlfr_ctx* ctx, float* d_feats)
 
 tlfr_status tlfr_route_labels(tlfr_ctx* ctx, float tol, float* d_labels, float* d_rgba)
 {
+    return tlfr_route_labels_ref(ctx, nullptr, tol, d_labels, d_rgba);
+}
+
+tlfr_status tlfr_route_labels_ref(tlfr_ctx* ctx, const float* d_ref, float tol, float* d_labels, float* d_rgba)
+{
     if (!ctx || !d_labels || !d_rgba || !(tol >= 0.0f))
         return fail(ctx, TLFR_BAD_ARG, "tlfr_route_labels: bad argument");
     tlfr::Ctx& c = ctx->c;
@@ -983,7 +988,8 @@ tlfr_status tlfr_route_labels(tlfr_ctx* ctx, float tol, float* d_labels, float* 
     if (st != TLFR_OK)
         return fail(ctx, st, "tlfr_route_labels: %s", c.error.c_str());
     std::string err;
-    st = tlfr::route_labels_from(c, reinterpret_cast<const float4*>(d_rgba), c.route_img, tol, d_labels, err);
+    st = tlfr::route_labels_from(c, reinterpret_cast<const float4*>(d_rgba), c.route_img,
+                                 reinterpret_cast<const float4*>(d_ref), tol, d_labels, err);
     if (st != TLFR_OK)
         return fail(ctx, st, "tlfr_route_labels: %s", err.c_str());
     cudaError_t e = cudaStreamSynchronize(c.stream);

@@ -223,8 +223,8 @@ tlfr_status route_predict(Route& r, const float* d_feats, long long n, float* d_
 tlfr_status route_probe(Ctx& c, int* d_counts);
 constexpr int kRouteProbes = 4;
 tlfr_status route_features(Ctx& c, float* d_feats, std::string& err);
-tlfr_status route_labels_from(Ctx& c, const float4* d_plain, const float4* d_fast, float tol, float* d_labels,
-                              std::string& err);
+tlfr_status route_labels_from(Ctx& c, const float4* d_plain, const float4* d_fast, const float4* d_ref, float tol,
+                              float* d_labels, std::string& err);
 tlfr_status route_flags(Ctx& c, const float* d_prob, float hi, unsigned char* d_fast, std::string& err);
 
 // build: reprojection, bucketing, kd split, leaf construction, emitNodes, top.

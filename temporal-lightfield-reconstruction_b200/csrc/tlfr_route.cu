@@ -1,8 +1,9 @@
 // tlfr_route.cu — learned routing (no counterpart in the reference: it is the
 // addition that sends easy pixels to a fast path).  The fast path is the plain
 // 1R pass that keeps the first surface when a second one opens instead of
-// refetching at 2R (light_scan_warp in tlfr_query.cu), so the expensive full
-// path runs only where the network is not confident.
+// refetching at 2R (light_scan_warp in tlfr_query.cu), on every second output
+// sample of the pixel's pattern, so the expensive full path runs only where the
+// network is not confident.
 //
 //   features   eight cheap per-pixel features: depth, depth range and CoC
 //              radius in the pixel, depth ranges within 3x3 and 5x5 tiles of
@@ -10,9 +11,11 @@
 //              nearest surface in that window is, motion magnitude, and a
 //              coarse pass: the plain 1R pass on four of the pixel's output
 //              samples, of which the fraction that needs the full path.
-//   labels     1 when the fast path reproduces the plain method's pixel
-//              within a tolerance on every channel (the plain method and the
-//              fast path are both run on the frame).
+//   labels     1 when the fast path is as good as the plain method at the
+//              pixel: within a tolerance of the plain pixel on every channel,
+//              or, given the scene's ground truth, with a squared error against
+//              it at most a tolerance above the plain pixel's (the plain method
+//              and the fast path are both run on the frame).
 //   network    8-64-64-1 MLP, ReLU, sigmoid output, binary cross-entropy.
 //              Forward, backward and inference run on the tensor cores
 //              (mma.sync m16n8k16, BF16 operands, FP32 accumulation); the
@@ -131,16 +134,30 @@ __global__ void k_feat_final(const float4* __restrict__ fa, const float4* __rest
     }
 }
 
-// Label 1 where the fast path reproduces the plain method's
-// pixel within tol on every channel.
-__global__ void k_labels(const float4* __restrict__ plain, const float4* __restrict__ fast, long long npix, float tol,
-                         float* __restrict__ labels)
+// Label 1 where the fast path is as good as the plain method: without a
+// reference image, where it reproduces the plain pixel within tol on every
+// channel; with one (the scene's ground truth), where its squared RGB error
+// against the reference exceeds the plain pixel's by at most tol.
+__global__ void k_labels(const float4* __restrict__ plain, const float4* __restrict__ fast,
+                         const float4* __restrict__ ref, long long npix, float tol, float* __restrict__ labels)
 {
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x)
     {
         const float4 a = plain[p], b = fast[p];
-        const float d = fmaxf(fmaxf(fabsf(a.x - b.x), fabsf(a.y - b.y)), fmaxf(fabsf(a.z - b.z), fabsf(a.w - b.w)));
-        labels[p] = d <= tol ? 1.0f : 0.0f;
+        bool ok;
+        if (ref)
+        {
+            const float4 r = ref[p];
+            const float ea = (a.x - r.x) * (a.x - r.x) + (a.y - r.y) * (a.y - r.y) + (a.z - r.z) * (a.z - r.z);
+            const float eb = (b.x - r.x) * (b.x - r.x) + (b.y - r.y) * (b.y - r.y) + (b.z - r.z) * (b.z - r.z);
+            ok = eb <= ea + tol;
+        }
+        else
+        {
+            const float d = fmaxf(fmaxf(fabsf(a.x - b.x), fabsf(a.y - b.y)), fmaxf(fabsf(a.z - b.z), fabsf(a.w - b.w)));
+            ok = d <= tol;
+        }
+        labels[p] = ok ? 1.0f : 0.0f;
     }
 }
 
@@ -714,12 +731,12 @@ tlfr_status route_features(Ctx& c, float* d_feats, std::string& err)
     return TLFR_OK;
 }
 
-tlfr_status route_labels_from(Ctx& c, const float4* d_plain, const float4* d_fast, float tol, float* d_labels,
-                              std::string& err)
+tlfr_status route_labels_from(Ctx& c, const float4* d_plain, const float4* d_fast, const float4* d_ref, float tol,
+                              float* d_labels, std::string& err)
 {
     const long long npix = (long long)c.W * c.H;
     const int blocks = (int)std::max(1LL, std::min((long long)c.num_sms * 16, (npix + 255) / 256));
-    k_labels<<<blocks, 256, 0, c.stream>>>(d_plain, d_fast, npix, tol, d_labels);
+    k_labels<<<blocks, 256, 0, c.stream>>>(d_plain, d_fast, d_ref, npix, tol, d_labels);
     c.launches++;
     CKR(cudaGetLastError());
     return TLFR_OK;

@@ -111,6 +111,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                                       ctypes.c_ulonglong, _FP]),
         "tlfr_route_features": (ctypes.c_int, [_VP, _VP]),
         "tlfr_route_labels": (ctypes.c_int, [_VP, ctypes.c_float, _VP, _VP]),
+        "tlfr_route_labels_ref": (ctypes.c_int, [_VP, _VP, ctypes.c_float, _VP, _VP]),
         "tlfr_router_create": (ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_uint, _FP, _FP, ctypes.POINTER(_VP)]),
         "tlfr_router_destroy": (None, [_VP]),
         "tlfr_router_last_error": (ctypes.c_char_p, [_VP]),
@@ -343,9 +344,15 @@ class TreeGather:
         """Eight routing features per pixel into device memory (W*H*8 floats)."""
         _check(load_library().tlfr_route_features(self._h, _VP(d_feats)), self._h)
 
-    def route_labels(self, d_labels: int, d_rgba: int, tol: float = 0.01):
-        """Plain reconstruction into d_rgba plus every pixel's label (fast path within tol of it)."""
-        _check(load_library().tlfr_route_labels(self._h, tol, _VP(d_labels), _VP(d_rgba)), self._h)
+    def route_labels(self, d_labels: int, d_rgba: int, tol: float = 0.01, d_ref: Optional[int] = None):
+        """Plain reconstruction into d_rgba plus every pixel's label: the fast path within tol of
+        the plain pixel, or (d_ref, a device ground-truth image) a squared error against d_ref
+        at most tol above the plain pixel's."""
+        if d_ref is None:
+            _check(load_library().tlfr_route_labels(self._h, tol, _VP(d_labels), _VP(d_rgba)), self._h)
+        else:
+            _check(load_library().tlfr_route_labels_ref(self._h, _VP(d_ref), tol, _VP(d_labels), _VP(d_rgba)),
+                   self._h)
 
     def set_routing(self, router: Optional["Router"], threshold: float = 0.8):
         """Learned routing on (router) or off (None) for the following reconstructions."""
