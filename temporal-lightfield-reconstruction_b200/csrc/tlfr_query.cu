@@ -62,8 +62,7 @@ struct QParams
     float c0, c1;               // refocused CoC coefficients
     float disp0;
     int   lens_filter, time_filter;
-    const unsigned char* route_fast;   // per pixel, nonzero: the router's fast path (or null)
-    int   route_mode;                  // light pass: kRouteAll, kRouteFull (skip fast pixels), kRouteFast
+    const unsigned char* route_fast;   // per pixel, nonzero: first-surface fast path (or null)
 };
 
 struct QStats
@@ -983,21 +982,13 @@ constexpr int kLightBlocksPerSM = 5;
 // Output sample ids q = pixel * M + i are unchanged (qcol, queues).
 enum { kMapLinear = 0, kMapTiles = 1 };
 constexpr int kTileW = 4, kTileH = 2, kTileSamples = 16;
-// Light-pass launches of a routed frame: kRouteFull takes the pixels the router
-// left on the plain method, kRouteFast the fast-path pixels, whose output
-// samples are every kFastStride-th of the pattern (the pattern is in (u,v,t)
-// Morton order, so the subset still spans the lens and the shutter), each
-// keeping the first surface instead of refetching at 2R.
-enum { kRouteAll = 0, kRouteFull = 1, kRouteFast = 2 };
-constexpr int kFastStride = 2;
 
 struct LightMap
 {
     int mode;
     long long units;        // block iterations
     int tiles_x;            // kMapTiles: tiles per row
-    int groups;             // kMapTiles: groups of 16 output samples per pixel (M / 16 / stride)
-    int stride;             // kMapTiles: output sample index step (kFastStride in the fast launch)
+    int groups;             // kMapTiles: groups of 16 output samples per pixel (M / 16)
 };
 
 // Output sample of thread t in block iteration u; false past the frame's end.
@@ -1014,7 +1005,7 @@ __device__ __forceinline__ bool light_query_id(const QParams& P, const LightMap&
     const int l = t & 31, p = l & 7;
     const int x = (int)(tile % L.tiles_x) * kTileW + (p & (kTileW - 1));
     const int y = (int)(tile / L.tiles_x) * kTileH + p / kTileW;
-    const int i = (g * kTileSamples + (t >> 5) * 4 + (l >> 3)) * L.stride;
+    const int i = g * kTileSamples + (t >> 5) * 4 + (l >> 3);
     q = ((long long)y * P.W + x) * P.M + i;
     return x < P.W && y < P.H;
 }
@@ -1033,13 +1024,11 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
     {
         // each lane: traversal and leaf sort of its own output sample
         long long q = 0;
-        bool valid = light_query_id(P, L, u, threadIdx.x, num_queries, q);
+        const bool valid = light_query_id(P, L, u, threadIdx.x, num_queries, q);
         Query o{};
         int nl = -2;
         const long long pix = valid ? (PROBE ? q / kProbe : q / P.M) : 0;
-        if (!PROBE && valid && P.route_mode != kRouteAll)
-            valid = (P.route_fast[pix] != 0) == (P.route_mode == kRouteFast);
-        const bool fast = !PROBE && valid && P.route_mode == kRouteFast;
+        const bool fast = !PROBE && valid && P.route_fast && P.route_fast[pix];
         if (valid)
         {
             o = PROBE ? make_query(P, (int)(pix % P.W), (int)(pix / P.W), (int)((q % kProbe) * P.M / kProbe))
@@ -1749,17 +1738,13 @@ k_query_overflow(QParams P, const int* __restrict__ queue, const int* __restrict
 
 // Pixel = sum of its output samples in sample order, times rcp(alpha); red
 // when empty (Reconstruction.cpp:665-719).
-// Fast-path pixels of a routed frame (route_fast set) sum every stride-th
-// output sample.
-__global__ void k_resolve(const float4* __restrict__ qcol, int M, float4* __restrict__ out, long long npix,
-                          const unsigned char* __restrict__ route_fast, int stride)
+__global__ void k_resolve(const float4* __restrict__ qcol, int M, float4* __restrict__ out, long long npix)
 {
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x)
     {
         const float4* c = qcol + p * M;
         float4 s = make_float4(0, 0, 0, 0);
-        const int step = (route_fast && route_fast[p]) ? stride : 1;
-        for (int i = 0; i < M; i += step)
+        for (int i = 0; i < M; i++)
         {
             const float4 v = c[i];
             s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
@@ -1818,7 +1803,6 @@ QParams make_params(const Ctx& c)
     P.lens_filter = c.params.lens_filter;
     P.time_filter = c.params.time_filter;
     P.route_fast = nullptr;
-    P.route_mode = kRouteAll;
     return P;
 }
 
@@ -1836,14 +1820,9 @@ size_t coop_scratch_bytes(int num_sms) { return sizeof(CoopScratch) * (size_t)nu
 
 // light pass iterations and lane map of a frame (nq_probe > 0: the router's
 // probe pass over nq_probe output samples, linear)
-// output sample step of the router's fast path (1 where the lane map cannot
-// subsample: M not a multiple of 16 * kFastStride)
-static int fast_stride(const Ctx& c) { return c.out_spp % (kTileSamples * kFastStride) == 0 ? kFastStride : 1; }
-
-static LightMap light_map(const Ctx& c, long long nq_probe = 0, int stride = 1)
+static LightMap light_map(const Ctx& c, long long nq_probe = 0)
 {
     LightMap L{};
-    L.stride = 1;
     if (nq_probe > 0 || c.out_spp % kTileSamples != 0)
     {
         const long long nq = nq_probe > 0 ? nq_probe : (long long)c.W * c.H * c.out_spp;
@@ -1852,35 +1831,10 @@ static LightMap light_map(const Ctx& c, long long nq_probe = 0, int stride = 1)
         return L;
     }
     L.mode = kMapTiles;
-    L.stride = stride;
     L.tiles_x = (c.W + kTileW - 1) / kTileW;
-    L.groups = c.out_spp / (kTileSamples * stride);
+    L.groups = c.out_spp / kTileSamples;
     L.units = (long long)L.tiles_x * ((c.H + kTileH - 1) / kTileH) * L.groups;
     return L;
-}
-
-// The light pass of a frame: one launch, or with router flags (P.route_fast)
-// the launch over the pixels left on the plain method and the fast-path launch
-// (all_fast: every pixel fast, the second launch alone).
-static void light_launches(Ctx& c, QParams P, int blocks, long long nq, cudaStream_t s, int* heavy_count,
-                           bool all_fast)
-{
-    if (!P.route_fast)
-    {
-        TLFR_LAUNCH(c, k_query_light<false>, blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
-                    heavy_count);
-        return;
-    }
-    if (!all_fast)
-    {
-        P.route_mode = kRouteFull;
-        TLFR_LAUNCH(c, k_query_light<false>, blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
-                    heavy_count);
-    }
-    P.route_mode = kRouteFast;
-    const LightMap F = light_map(c, 0, fast_stride(c));
-    TLFR_LAUNCH(c, k_query_light<false>, (int)std::min<long long>(F.units, (long long)blocks), kBlock, s, P, F, nq,
-                c.qcol, c.heavy_queue, heavy_count);
 }
 size_t overflow_scratch_bytes() { return slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf) * kOvSlots; }
 
@@ -1988,14 +1942,15 @@ tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_bloc
         c.launches++;
         P.route_fast = c.route_fast;
     }
-    light_launches(c, P, light_blocks, nq, s, counters + 2, false);
+    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
+                counters + 2);
     TLFR_LAUNCH(c, k_query_coop, coop_blocks(c), kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol, c.ovf_queue,
                 counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(coop_scratch));
     TLFR_LAUNCH(c, k_query_overflow, kOvSlots / 64, 64, s, P, c.ovf_queue, counters + 0, (int)c.ovf_cap, c.qcol,
                 (char*)ovf_scratch, slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf), kOvSlots, kOvStack, kOvLeaf,
                 kOvRs, kOvSurf, counters + 1, c.d_stats, 0);
     TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, (long long)c.num_sms * 32), 128, s, c.qcol,
-                c.out_spp, d_rgba, npix, P.route_fast, fast_stride(c));
+                c.out_spp, d_rgba, npix);
     c.stream = saved;
     CKQ(cudaGetLastError());
     return TLFR_OK;
@@ -2109,7 +2064,8 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
             c.coop_scratch_bytes = coop_scratch_bytes(c.num_sms);
             CKQ(cudaMalloc(&c.coop_scratch, c.coop_scratch_bytes));
         }
-        light_launches(c, P, light_default_blocks(c), nq, s, counters + 2, c.route_all_fast);
+        TLFR_LAUNCH(c, k_query_light<false>, light_default_blocks(c), kBlock, s, P, light_map(c), nq, c.qcol,
+                    c.heavy_queue, counters + 2);
         CKQ(cudaEventRecord(c.evq1, s));
         TLFR_LAUNCH(c, k_query_coop, coop_blocks(c), kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol,
                     c.ovf_queue, counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(c.coop_scratch));
@@ -2143,7 +2099,7 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
         CKQ(cudaMemcpyAsync(&hard, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     }
     TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, (long long)c.num_sms * 32), 128, s, c.qcol,
-                c.out_spp, d_rgba, npix, collect_stats ? nullptr : P.route_fast, fast_stride(c));
+                c.out_spp, d_rgba, npix);
     CKQ(cudaGetLastError());
     {
         float ms = 0, ms2 = 0;

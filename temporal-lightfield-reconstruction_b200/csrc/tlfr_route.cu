@@ -1,9 +1,8 @@
 // tlfr_route.cu — learned routing (no counterpart in the reference: it is the
 // addition that sends easy pixels to a fast path).  The fast path is the plain
 // 1R pass that keeps the first surface when a second one opens instead of
-// refetching at 2R (light_scan_warp in tlfr_query.cu), on every second output
-// sample of the pixel's pattern, so the expensive full path runs only where the
-// network is not confident.
+// refetching at 2R (light_scan_warp in tlfr_query.cu), so the expensive full
+// path runs only where the network is not confident.
 //
 //   features   eight cheap per-pixel features: depth, depth range and CoC
 //              radius in the pixel, depth ranges within 3x3 and 5x5 tiles of
