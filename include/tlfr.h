@@ -179,6 +179,14 @@ tlfr_status tlfr_tree_export(tlfr_ctx* ctx, float* nodef, int* nodei, float* sam
  * (generateOutputSamples, Reconstruction.cpp:452-512).  Returns the entry count.  */
 int tlfr_output_samples(tlfr_ctx* ctx, float* out5);
 
+/* The output samples of the last reconstruction as a sample buffer
+ * (Reconstruction.cpp:290-294, 696-712: the m_obuf debug dump, which the
+ * reference writes with UVTSampleBuffer::serialize): W*H*M records, record
+ * (x, y, i) holding the output sample's x, y, u, v, t and its reconstructed
+ * RGBA; z/w = w = 1 and no motion.  Save it with tlfr_buffer_save; free it
+ * with tlfr_buffer_free.                                                     */
+tlfr_status tlfr_output_sample_buffer(tlfr_ctx* ctx, tlfr_buffer** out);
+
 /* Run the output samples (x, y, i) listed in xyi[3*k ..] through the device query
  * path with tracing on.  rgba[4*k ..] = the query colour.  trace[k*trace_stride ..]:
  *   [0] flags: bit0 = 2R fetch, bit1 = widened beyond 2R, bit2 = surfaces merged,

@@ -910,6 +910,56 @@ int tlfr_output_samples(tlfr_ctx* ctx, float* out5)
     return (int)(ctx->c.h_pattern.size() / 5);
 }
 
+// The reconstruction's output-sample buffer (the m_obuf debug dump,
+// Reconstruction.cpp:290-294, 696-712): one record per output sample (x, y, i)
+// with the sample's position, lens and time coordinates and its reconstructed
+// colour, the rest of the record as a fresh buffer holds it (w = 1, no motion).
+tlfr_status tlfr_output_sample_buffer(tlfr_ctx* ctx, tlfr_buffer** out)
+{
+    if (!ctx || !out)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_output_sample_buffer: bad argument");
+    tlfr::Ctx& c = ctx->c;
+    const int M = c.out_spp;
+    const size_t n = (size_t)c.W * c.H * M;
+    if (!c.qcol || c.qcol_cap < n)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_output_sample_buffer: no reconstruction yet");
+    cudaSetDevice(c.device);
+    std::vector<float> col(4 * n);
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(col.data(), c.qcol, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return fail(ctx, TLFR_CUDA, "tlfr_output_sample_buffer: %s", cudaGetErrorString(e));
+    tlfr_buffer* b = new (std::nothrow) tlfr_buffer();
+    if (!b)
+        return fail(ctx, TLFR_OOM, "host allocation failed");
+    b->W = c.W; b->H = c.H; b->spp = M;
+    b->coc[0] = c.coc[0]; b->coc[1] = c.coc[1];
+    if (!b->alloc(n))
+    {
+        delete b;
+        return fail(ctx, TLFR_OOM, "host allocation failed");
+    }
+    for (int y = 0; y < c.H; y++)
+        for (int x = 0; x < c.W; x++)
+        {
+            const int pattern = (int)(tlfr::hash_bits((uint32_t)x, (uint32_t)y) % 64u);
+            for (int i = 0; i < M; i++)
+            {
+                const size_t k = ((size_t)y * c.W + x) * M + i;
+                const float* o = &c.h_pattern[((size_t)pattern * M + i) * 5];
+                float* r = b->rec + 16 * k;
+                r[0] = o[0] + (float)x; r[1] = o[1] + (float)y;
+                r[2] = 1.0f; r[3] = 1.0f;
+                r[4] = o[2]; r[5] = o[3]; r[6] = o[4];
+                r[7] = col[4 * k]; r[8] = col[4 * k + 1]; r[9] = col[4 * k + 2]; r[10] = col[4 * k + 3];
+                r[11] = r[12] = r[13] = r[14] = r[15] = 0.0f;
+            }
+        }
+    *out = b;
+    return TLFR_OK;
+}
+
 tlfr_status tlfr_query_samples_noalloc(tlfr_ctx* ctx, const int* d_xyi, int n, float* d_rgba, int* d_overflow)
 {
     if (!ctx || (n > 0 && (!d_xyi || !d_rgba)))

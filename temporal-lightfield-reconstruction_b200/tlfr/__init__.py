@@ -105,6 +105,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_output_samples": (ctypes.c_int, [_VP, _FP]),
         "tlfr_trace_queries": (ctypes.c_int, [_VP, _IP, ctypes.c_int, _FP, _IP, ctypes.c_int]),
         "tlfr_query_samples_noalloc": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
+        "tlfr_output_sample_buffer": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
         "tlfr_synth_scene": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_ulonglong, _FP, _FP]),
         "tlfr_synth_reference_image": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -186,6 +187,12 @@ class UVTSampleBuffer:
                 height, width, spp = rec.shape[:3]
             _check(lib.tlfr_buffer_from_host(_f32p(rec), width, height, spp, coc[0], coc[1], ctypes.byref(h)))
         self._h = h
+
+    @classmethod
+    def _from_handle(cls, h) -> "UVTSampleBuffer":
+        b = cls.__new__(cls)
+        b._h = h
+        return b
 
     @property
     def handle(self):
@@ -331,6 +338,13 @@ class TreeGather:
         out = np.zeros((n, 5), np.float32)
         load_library().tlfr_output_samples(self._h, _f32p(out))
         return out
+
+    def output_sample_buffer(self) -> "UVTSampleBuffer":
+        """The last reconstruction's output samples as a sample buffer (the reference's
+        m_obuf dump, Reconstruction.cpp:290-294, 696-712)."""
+        h = _VP()
+        _check(load_library().tlfr_output_sample_buffer(self._h, ctypes.byref(h)), self._h)
+        return UVTSampleBuffer._from_handle(h)
 
     def trace_queries(self, xyi: Sequence[Tuple[int, int, int]], stride: int = 4096):
         q = np.ascontiguousarray(np.asarray(xyi, np.int32).reshape(-1, 3))

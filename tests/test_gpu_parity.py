@@ -215,3 +215,33 @@ def test_gpu_full_frame_matches_oracle(name, preset, W, H, spp, seed, p):
     ref = o.reconstruct()
     assert rel_err(img, ref).max() <= RTOL
     assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+
+
+def test_gpu_output_sample_buffer_matches_oracle(tmp_path):
+    """The output-sample dump (the reference's m_obuf): every record holds its
+    output sample's position, lens and time coordinates and the colour the oracle
+    computes for it; the dump survives a text save and load."""
+    W, H, spp = 24, 16, 4
+    rec, coc = tlfr.synth_scene(tlfr.SCENE_CARDS, W, H, spp, 42)
+    g = gpu_recon(rec, coc)
+    g.reconstructDofMotion()
+    ob = g.output_sample_buffer()
+    M = 128
+    r = ob.records()
+    assert r.shape == (H, W, M, 16)
+    o = CpuRecon("orc", rec, coc)
+    pat = o.output_samples().reshape(64, M, 5)
+    from tlfr_testutil import hash_pattern
+    rng = np.random.default_rng(43)
+    for _ in range(200):
+        x, y, i = int(rng.integers(0, W)), int(rng.integers(0, H)), int(rng.integers(0, M))
+        pp = pat[hash_pattern(x, y), i]
+        want = np.float32([pp[0] + x, pp[1] + y, 1, 1, pp[2], pp[3], pp[4]])
+        assert np.array_equal(r[y, x, i, :7].view(np.uint32), want.view(np.uint32))
+        col, _ = o.query(x, y, i)
+        assert np.array_equal(r[y, x, i, 7:11].view(np.uint32), col.view(np.uint32))
+    path = str(tmp_path / "outputSamples.txt")
+    ob.serialize(path, separate_header=False, binary=False)
+    back = tlfr.UVTSampleBuffer(path).records()
+    # text round trip keeps positions and colours (alpha is forced to 1 on load)
+    assert np.allclose(back[..., :10], r[..., :10], rtol=1e-6, atol=1e-6)

@@ -216,3 +216,20 @@ def sample_queries(W, H, M, n, seed=0):
 
 def rel_err(a, b, floor=1e-6):
     return np.abs(a - b) / np.maximum(np.abs(b), floor)
+
+
+def hash_pattern(x, y):
+    """Output pattern of pixel (x, y): hashBits(x, y) % 64 (Hash.hpp:169-183,
+    Reconstruction.cpp:653)."""
+    m = 0xffffffff
+    a, b, c = x & m, y & m, 0x9e3779b9
+    a = (a - b) & m; a = (a - c) & m; a ^= (c >> 13)
+    b = (b - c) & m; b = (b - a) & m; b = (b ^ (a << 8)) & m
+    c = (c - a) & m; c = (c - b) & m; c ^= (b >> 13)
+    a = (a - b) & m; a = (a - c) & m; a ^= (c >> 12)
+    b = (b - c) & m; b = (b - a) & m; b = (b ^ (a << 16)) & m
+    c = (c - a) & m; c = (c - b) & m; c ^= (b >> 5)
+    a = (a - b) & m; a = (a - c) & m; a ^= (c >> 3)
+    b = (b - c) & m; b = (b - a) & m; b = (b ^ (a << 10)) & m
+    c = (c - a) & m; c = (c - b) & m; c ^= (b >> 15)
+    return c % 64
