@@ -73,7 +73,7 @@ def parse():
                     help="label tolerance: squared RGB error above the plain pixel's (gt) or channel difference")
     ap.add_argument("--gt-samples", type=int, default=1024, help="ground-truth samples per pixel")
     ap.add_argument("--batch-frames", type=int, default=48, help="uneven-buffer batch size (0: no batch run)")
-    ap.add_argument("--batch-scale", type=int, default=4, help="linear downscale of the batch's resolutions")
+    ap.add_argument("--batch-scale", type=int, default=1, help="linear downscale of the batch's resolutions")
     ap.add_argument("--profile-frame", action="store_true",
                     help="time the query passes of one frame (--width/--height/--spp, --steps/--warmup) and print "
                          "one JSON line; the entry point for profiler captures")
@@ -404,7 +404,8 @@ def run_batch(args, device, router, steps, warmup):
     for _ in range(steps):
         batch.run()
         ms.append(batch.sync())
-    blocks = batch.light_blocks()
+    shapes = batch.tile_shapes()
+    chunks, launches = batch.layout()
     batch.close()
     for g in trees:
         g.close()
@@ -415,8 +416,10 @@ def run_batch(args, device, router, steps, warmup):
                   f"router {'on' if router is not None else 'off'}",
         "frames": args.batch_frames, "pixels": pix, "output_samples": pix * 128,
         "value": pix / (t / 1e3) / 1e6, "unit": "Mpix/s", "ms_per_run": t, "runs": steps,
-        "create_s": create_s, "light_grid_blocks": sorted(set(int(b) for b in blocks)),
-        "launch": "one CUDA graph per run",
+        "create_s": create_s,
+        "tile_shapes": {tlfr.TILE_SHAPES[k]: int((shapes == k).sum()) for k in sorted(set(int(x) for x in shapes))},
+        "chunks": int(chunks.max()) + 1, "launches_per_run": int(launches),
+        "launch": "one CUDA graph per run; per chunk one persistent launch per pass over all its frames",
     }
 
 

@@ -291,17 +291,35 @@ tlfr_status tlfr_router_set_params(tlfr_router* router, const float* params);
 tlfr_status tlfr_set_routing(tlfr_ctx* ctx, tlfr_router* router, float threshold);
 
 /* ---- batches -----------------------------------------------------------------
- * Many built contexts (sample buffers of any resolution and spp) reconstructed
- * as one CUDA graph replayed on one stream: each frame's router (if set),
- * light pass, cooperative full-path pass, large-capacity pass and pixel resolve,
- * with no host synchronisation inside.  With autotune, each frame's light-pass
- * grid (resident blocks per SM) is chosen by timing candidates at creation.
- * Replaces the reference's per-frame reconstruct loop of the animation/export
- * paths (reconstruction_app/App.cpp:616-694).  The graph holds the contexts'
- * buffers as they are at creation: after rebuilding a context with records of
- * another size, create the batch again.  The contexts (and a router set on one)
- * must outlive the batch.  Outputs are device RGBA float images. */
+ * Many frames reconstructed as one CUDA graph replayed on one stream, with no
+ * host synchronisation inside.  A frame is a built context (a sample buffer of
+ * any resolution and spp) with either its own output settings or, for sweeps
+ * over one hierarchy, output settings of the frame's own (override_uvt / uvt,
+ * output_spp, lens and time filters; aperture and focus adjustments change the
+ * hierarchy and need a context of their own).  Each pass runs as ONE persistent
+ * launch over all frames of a chunk: blocks take work items (frame, unit) from
+ * a device counter and read the frame's parameters from a device table.
+ * Frames are grouped into chunks whose per-output-sample storage (24 bytes per
+ * output sample) fits budget_bytes (0: half the free device memory, at most
+ * 32 GiB); chunks run one after another and share the storage.  With autotune,
+ * each frame's light-pass tile shape is chosen by timing every shape at
+ * creation.  A frame's router (set on its context, own output settings only)
+ * runs before its chunk.  Replaces the reference's per-frame reconstruct loops
+ * of the animation and export paths (reconstruction_app/App.cpp:616-694,
+ * a new TreeGather per (u,v) frame).  The graph holds the contexts' buffers as
+ * they are at creation: after rebuilding a context with records of another
+ * size, create the batch again.  The contexts (and routers) must outlive the
+ * batch.  Outputs are device RGBA float images. */
 typedef struct tlfr_batch tlfr_batch;
+typedef struct tlfr_batch_frame
+{
+    tlfr_ctx*          ctx;
+    const tlfr_params* output;     /* NULL: the context's own output settings */
+    float*             d_rgba;     /* device RGBA image, width*height*4 floats */
+} tlfr_batch_frame;
+tlfr_status tlfr_batch_create_frames(const tlfr_batch_frame* frames, int n, void* stream, int autotune,
+                                     size_t budget_bytes, tlfr_batch** out);
+/* The same for n contexts with their own output settings and the default budget. */
 tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba, void* stream, int autotune,
                               tlfr_batch** out);
 /* Replays the batch on its stream (asynchronous). */
@@ -309,8 +327,11 @@ tlfr_status tlfr_batch_run(tlfr_batch* batch);
 /* Waits for the last run; device time in ms (optional); TLFR_OVERFLOW when an
  * output sample exceeded every capacity. */
 tlfr_status tlfr_batch_sync(tlfr_batch* batch, double* ms);
-/* The light-pass grid chosen for each frame (n entries). */
-tlfr_status tlfr_batch_info(const tlfr_batch* batch, int* light_blocks);
+/* The light-pass tile shape chosen for each frame (n entries): 0 = 4x2 pixels
+ * x 4 output samples per warp, 1 = 8x4 x 1, 2 = 4x4 x 2, 3 = 2x2 x 8, 4 = 2x1 x 16. */
+tlfr_status tlfr_batch_info(const tlfr_batch* batch, int* tile_shapes);
+/* The chunk of each frame (n entries, optional) and the kernel launches of one run. */
+tlfr_status tlfr_batch_layout(const tlfr_batch* batch, int* chunks, long long* launches);
 const char* tlfr_batch_last_error(const tlfr_batch* batch);
 void        tlfr_batch_destroy(tlfr_batch* batch);
 

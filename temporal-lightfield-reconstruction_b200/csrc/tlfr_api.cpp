@@ -1167,16 +1167,15 @@ tlfr_status tlfr_set_routing(tlfr_ctx* ctx, tlfr_router* r, float threshold)
 struct tlfr_batch
 {
     std::vector<tlfr_ctx*> ctx;
-    std::vector<float*> out;
-    std::vector<int> light_blocks;
+    tlfr::BatchPlan* plan = nullptr;
+    std::vector<tlfr_params> outputs;   // per-frame output settings (kept alive for the plan)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int device = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    void* coop_scratch = nullptr;   // working storage of the full-path passes, shared by the
-    void* ovf_scratch = nullptr;    // batch's frames (they run one after another on its stream)
+    long long launches = 0;             // kernel launches of one run
     std::string error;
 };
 
@@ -1196,30 +1195,44 @@ static void batch_free(tlfr_batch* b)
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
-    if (b->coop_scratch) cudaFree(b->coop_scratch);
-    if (b->ovf_scratch) cudaFree(b->ovf_scratch);
+    tlfr::batch_plan_delete(b->plan);
     delete b;
 }
 
-tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba, void* stream, int autotune,
-                              tlfr_batch** out)
+tlfr_status tlfr_batch_create_frames(const tlfr_batch_frame* frames, int n, void* stream, int autotune,
+                                     size_t budget_bytes, tlfr_batch** out)
 {
-    if (!ctxs || !d_rgba || n <= 0 || !out)
+    if (!frames || n <= 0 || !out)
         return batch_fail(nullptr, TLFR_BAD_ARG, "tlfr_batch_create: bad argument");
     for (int i = 0; i < n; i++)
-        if (!ctxs[i] || !d_rgba[i])
+        if (!frames[i].ctx || !frames[i].d_rgba)
             return batch_fail(nullptr, TLFR_BAD_ARG, "tlfr_batch_create: null context or output " + std::to_string(i));
-    const int dev = ctxs[0]->c.device;
+    const int dev = frames[0].ctx->c.device;
     for (int i = 1; i < n; i++)
-        if (ctxs[i]->c.device != dev)
+        if (frames[i].ctx->c.device != dev)
             return batch_fail(nullptr, TLFR_BAD_ARG, "tlfr_batch_create: contexts on different devices");
     cudaSetDevice(dev);
     tlfr_batch* b = new (std::nothrow) tlfr_batch;
     if (!b)
         return batch_fail(nullptr, TLFR_OOM, "host allocation failed");
     b->device = dev;
-    b->ctx.assign(ctxs, ctxs + n);
-    b->out.assign(d_rgba, d_rgba + n);
+    b->plan = tlfr::batch_plan_new();
+    if (!b->plan)
+    {
+        delete b;
+        return batch_fail(nullptr, TLFR_OOM, "host allocation failed");
+    }
+    b->outputs.resize(n);
+    std::vector<tlfr::BatchEntry> entries(n);
+    for (int i = 0; i < n; i++)
+    {
+        b->ctx.push_back(frames[i].ctx);
+        if (frames[i].output)
+            b->outputs[i] = *frames[i].output;
+        entries[i].ctx = &frames[i].ctx->c;
+        entries[i].output = frames[i].output ? &b->outputs[i] : nullptr;
+        entries[i].out = reinterpret_cast<float4*>(frames[i].d_rgba);
+    }
     b->stream = static_cast<cudaStream_t>(stream);
     if (!b->stream)
     {
@@ -1235,76 +1248,37 @@ tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba
         batch_free(b);
         return batch_fail(nullptr, TLFR_CUDA, m);
     };
-    // shared working storage, each frame's buffers, the light pass's grid per
-    // frame, one eager run (lazy scratch of the router), then the capture
+    if (budget_bytes == 0)
     {
-        cudaError_t e = cudaMalloc(&b->coop_scratch, tlfr::coop_scratch_bytes(ctxs[0]->c.num_sms));
-        if (e == cudaSuccess)
-            e = cudaMalloc(&b->ovf_scratch, tlfr::overflow_scratch_bytes());
-        if (e != cudaSuccess)
-        {
-            batch_free(b);
-            return batch_fail(nullptr, TLFR_OOM, std::string("tlfr_batch_create: scratch: ") + cudaGetErrorString(e));
-        }
+        // default: half of the free device memory, at most 32 GiB
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        budget_bytes = std::min<size_t>(fr / 2, (size_t)32 << 30);
     }
-    for (int i = 0; i < n; i++)
+    std::string err;
+    tlfr_status st = tlfr::batch_build(*b->plan, entries, b->stream, autotune != 0, budget_bytes, err);
+    if (st != TLFR_OK)
     {
-        tlfr::Ctx& c = b->ctx[i]->c;
-        tlfr_status st = tlfr::frame_prepare(c, false);
-        if (st != TLFR_OK)
-        {
-            const std::string m = "tlfr_batch_create: frame " + std::to_string(i) + ": " + c.error;
-            batch_free(b);
-            return batch_fail(nullptr, st, m);
-        }
-        int best = tlfr::light_default_blocks(c);
-        if (autotune)
-        {
-            // persistent grids of k resident 128-thread blocks per SM, k = 2..32
-            const int cap = best;
-            float best_ms = 1e30f;
-            for (int k : { 2, 4, 8, 16, 32 })
-            {
-                const int blocks = std::min(cap, c.num_sms * k);
-                float ms = 0;
-                st = tlfr::light_trial(c, b->stream, blocks, &ms);
-                if (st != TLFR_OK)
-                {
-                    const std::string m = "tlfr_batch_create: autotune: " + c.error;
-                    batch_free(b);
-                    return batch_fail(nullptr, st, m);
-                }
-                if (ms < best_ms)
-                {
-                    best_ms = ms;
-                    best = blocks;
-                }
-            }
-        }
-        b->light_blocks.push_back(best);
+        batch_free(b);
+        return batch_fail(nullptr, st, "tlfr_batch_create: " + err);
     }
+    // one eager run (lazy scratch of the router), then the capture
     for (int pass = 0; pass < 2; pass++)
     {
         cudaError_t e = cudaSuccess;
         if (pass == 1 && (e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
             return cuda_fail("cudaStreamBeginCapture", e);
-        for (int i = 0; i < n; i++)
+        st = tlfr::batch_enqueue(*b->plan, b->stream, err, &b->launches);
+        if (st != TLFR_OK)
         {
-            tlfr::Ctx& c = b->ctx[i]->c;
-            tlfr_status st = tlfr::frame_enqueue(c, reinterpret_cast<float4*>(b->out[i]), b->stream, b->light_blocks[i],
-                                                 b->coop_scratch, b->ovf_scratch);
-            if (st != TLFR_OK)
+            if (pass == 1)
             {
-                if (pass == 1)
-                {
-                    cudaGraph_t g = nullptr;
-                    cudaStreamEndCapture(b->stream, &g);
-                    if (g) cudaGraphDestroy(g);
-                }
-                const std::string m = "tlfr_batch_create: frame " + std::to_string(i) + ": " + c.error;
-                batch_free(b);
-                return batch_fail(nullptr, st, m);
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(b->stream, &g);
+                if (g) cudaGraphDestroy(g);
             }
+            batch_free(b);
+            return batch_fail(nullptr, st, "tlfr_batch_create: " + err);
         }
         if (pass == 0 && (e = cudaStreamSynchronize(b->stream)) != cudaSuccess)
             return cuda_fail("warm-up run", e);
@@ -1320,6 +1294,17 @@ tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba
         return cuda_fail("cudaEventCreate", cudaGetLastError());
     *out = b;
     return TLFR_OK;
+}
+
+tlfr_status tlfr_batch_create(tlfr_ctx* const* ctxs, int n, float* const* d_rgba, void* stream, int autotune,
+                              tlfr_batch** out)
+{
+    if (!ctxs || !d_rgba || n <= 0 || !out)
+        return batch_fail(nullptr, TLFR_BAD_ARG, "tlfr_batch_create: bad argument");
+    std::vector<tlfr_batch_frame> fr(n);
+    for (int i = 0; i < n; i++)
+        fr[i] = tlfr_batch_frame{ ctxs[i], nullptr, d_rgba[i] };
+    return tlfr_batch_create_frames(fr.data(), n, stream, autotune, 0, out);
 }
 
 tlfr_status tlfr_batch_run(tlfr_batch* b)
@@ -1351,24 +1336,33 @@ tlfr_status tlfr_batch_sync(tlfr_batch* b, double* ms)
         cudaEventElapsedTime(&f, b->ev0, b->ev1);
         *ms = f;
     }
-    for (size_t i = 0; i < b->ctx.size(); i++)
-    {
-        int hard = 0;
-        if (tlfr::frame_hard_failures(b->ctx[i]->c, b->stream, &hard) != TLFR_OK)
-            return batch_fail(b, TLFR_CUDA, "tlfr_batch_sync: " + b->ctx[i]->c.error);
-        if (hard > 0)
+    std::vector<int> hard;
+    std::string err;
+    if (tlfr::batch_failures(*b->plan, b->stream, hard, err) != TLFR_OK)
+        return batch_fail(b, TLFR_CUDA, "tlfr_batch_sync: " + err);
+    for (size_t i = 0; i < hard.size(); i++)
+        if (hard[i] > 0)
             return batch_fail(b, TLFR_OVERFLOW, "tlfr_batch_sync: frame " + std::to_string(i) +
                                                     ": a query exceeded the largest supported capacity");
-    }
     return TLFR_OK;
 }
 
-tlfr_status tlfr_batch_info(const tlfr_batch* b, int* light_blocks)
+tlfr_status tlfr_batch_info(const tlfr_batch* b, int* tile_shapes)
 {
-    if (!b || !light_blocks)
+    if (!b || !tile_shapes)
         return TLFR_BAD_ARG;
-    for (size_t i = 0; i < b->light_blocks.size(); i++)
-        light_blocks[i] = b->light_blocks[i];
+    tlfr::batch_info(*b->plan, tile_shapes, nullptr);
+    return TLFR_OK;
+}
+
+tlfr_status tlfr_batch_layout(const tlfr_batch* b, int* chunks, long long* launches)
+{
+    if (!b)
+        return TLFR_BAD_ARG;
+    if (chunks)
+        tlfr::batch_info(*b->plan, nullptr, chunks);
+    if (launches)
+        *launches = b->launches;
     return TLFR_OK;
 }
 

@@ -231,18 +231,25 @@ tlfr_status route_flags(Ctx& c, const float* d_prob, float hi, unsigned char* d_
 tlfr_status build_hierarchy(Ctx& c, const float* d_records);
 // query: all output samples of the frame into rgba (device pointer).
 tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats);
-// the same with no host synchronisation (batches, CUDA graph capture)
-// own_scratch: allocate the context's own working storage of the full-path
-// passes; batches pass one shared set to frame_enqueue instead (null: the
-// context's own)
-tlfr_status frame_prepare(Ctx& c, bool own_scratch);
-tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_blocks, void* coop_scratch,
-                          void* ovf_scratch);
-size_t coop_scratch_bytes(int num_sms);
-size_t overflow_scratch_bytes();
-tlfr_status frame_hard_failures(Ctx& c, cudaStream_t s, int* hard);
-tlfr_status light_trial(Ctx& c, cudaStream_t s, int light_blocks, float* ms);
+// Batches (tlfr_query.cu): frames reconstructed together in one CUDA graph with
+// one persistent launch per pass per chunk of frames.
+struct BatchEntry
+{
+    Ctx* ctx;
+    const tlfr_params* output;      // the frame's own output settings (null: the context's)
+    float4* out;                    // device pixels
+};
+struct BatchPlan;
+BatchPlan* batch_plan_new();
+void batch_plan_delete(BatchPlan* bp);
+tlfr_status batch_build(BatchPlan& bp, const std::vector<BatchEntry>& entries, cudaStream_t s, bool autotune,
+                        size_t budget, std::string& err);
+tlfr_status batch_enqueue(BatchPlan& bp, cudaStream_t s, std::string& err, long long* launches);
+tlfr_status batch_failures(BatchPlan& bp, cudaStream_t s, std::vector<int>& hard, std::string& err);
+void batch_info(const BatchPlan& bp, int* shapes, int* chunks);
 int light_default_blocks(const Ctx& c);
+size_t overflow_scratch_bytes();
+size_t coop_scratch_bytes(int num_sms);
 tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h_trace, int stride);
 // output samples through the full path with working storage in a fixed device array
 tlfr_status query_samples_noalloc(Ctx& c, const int* d_xyi, int n, float* d_rgba, int* d_overflow);

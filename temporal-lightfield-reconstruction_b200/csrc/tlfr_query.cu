@@ -29,6 +29,7 @@
 #include "tlfr_common.cuh"
 #include "tlfr_internal.h"
 
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -972,24 +973,30 @@ constexpr int kLightBlocksPerSM = 5;
 // a pixel are spread over the whole lens and shutter (the reference sorts each
 // pattern's samples by a (u,v,t) Morton key, Reconstruction.cpp:484-510, so
 // sample i of every pattern sits near the same place on that curve):
-//   kMapTiles (M a multiple of 16): an iteration of a block covers a 4x2-pixel
-//     tile and 16 consecutive output samples of each of its pixels; warp w takes
-//     samples 4w..4w+3 of the group, lane l pixel l % 8 and sample l / 8.  The
-//     union of the hierarchy nodes a warp reaches is 3.8x one output sample's
-//     (5.3x for a pixel's 32 consecutive samples) at 1920x1080x8.
+//   kMapTiles: a warp takes a tile of tw x th pixels (px = tw*th lanes per
+//     sample) and sw = 32/px consecutive output samples of each; a block
+//     iteration covers the tile and 4*sw consecutive samples (its four warps).
+//     The default tile is 4x2 pixels x 4 samples: the union of the hierarchy
+//     nodes a warp reaches is then 3.8x one output sample's at 1920x1080x8
+//     (5.3x for a pixel's 32 consecutive samples); batches choose the shape
+//     per frame by timing (autotuner).
 //   kMapLinear: q = block iteration * 128 + thread (the pinhole image's one
-//     sample per pixel, and M not a multiple of 16).
+//     sample per pixel, and M not a multiple of 4*sw).
 // Output sample ids q = pixel * M + i are unchanged (qcol, queues).
 enum { kMapLinear = 0, kMapTiles = 1 };
-constexpr int kTileW = 4, kTileH = 2, kTileSamples = 16;
 
 struct LightMap
 {
     int mode;
     long long units;        // block iterations
+    int tw, th, sw;         // kMapTiles: tile width and height (pixels), output samples per lane column
     int tiles_x;            // kMapTiles: tiles per row
-    int groups;             // kMapTiles: groups of 16 output samples per pixel (M / 16)
+    int groups;             // kMapTiles: groups of 4*sw output samples per pixel (M / (4*sw))
 };
+
+// tile shapes the autotuner tries: (tw, th), sw = 32 / (tw*th)
+constexpr int kTileShapes[5][2] = { { 4, 2 }, { 8, 4 }, { 4, 4 }, { 2, 2 }, { 2, 1 } };
+constexpr int kDefaultShape = 0;
 
 // Output sample of thread t in block iteration u; false past the frame's end.
 __device__ __forceinline__ bool light_query_id(const QParams& P, const LightMap& L, long long u, int t,
@@ -1002,25 +1009,32 @@ __device__ __forceinline__ bool light_query_id(const QParams& P, const LightMap&
     }
     const long long tile = u / L.groups;
     const int g = (int)(u - tile * L.groups);
-    const int l = t & 31, p = l & 7;
-    const int x = (int)(tile % L.tiles_x) * kTileW + (p & (kTileW - 1));
-    const int y = (int)(tile / L.tiles_x) * kTileH + p / kTileW;
-    const int i = g * kTileSamples + (t >> 5) * 4 + (l >> 3);
+    const int px = L.tw * L.th;
+    const int l = t & 31, p = l % px;
+    const int x = (int)(tile % L.tiles_x) * L.tw + p % L.tw;
+    const int y = (int)(tile / L.tiles_x) * L.th + p / L.tw;
+    const int i = (g * 4 + (t >> 5)) * L.sw + l / px;
     q = ((long long)y * P.W + x) * P.M + i;
     return x < P.W && y < P.H;
 }
 
-template <bool PROBE>
-__global__ void __launch_bounds__(kBlock, kLightBlocksPerSM)
-k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
-              int* __restrict__ heavy_count)
+// Shared-memory columns of a light-pass block.
+struct LightShared
 {
-    __shared__ float2 sh_leaves[kLLeaf][kBlock];
-    __shared__ int sh_stack[kLStack][kBlock];
+    float2 leaves[kLLeaf][kBlock];
+    int stack[kLStack][kBlock];
+};
+
+// One block iteration u of the light pass.
+template <bool PROBE>
+__device__ __forceinline__ void light_unit(const QParams& P, const LightMap& L, long long u, long long num_queries,
+                                           float4* __restrict__ qcol, int* __restrict__ heavy,
+                                           int* __restrict__ heavy_count, LightShared& sh)
+{
+    float2 (&sh_leaves)[kLLeaf][kBlock] = sh.leaves;
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
-    const Column<int> stack{ &sh_stack[0][threadIdx.x], kBlock };
-    for (long long u = blockIdx.x; u < L.units; u += gridDim.x)
+    const Column<int> stack{ &sh.stack[0][threadIdx.x], kBlock };
     {
         // each lane: traversal and leaf sort of its own output sample
         long long q = 0;
@@ -1066,7 +1080,7 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
             // heavy_count is the per-pixel count here
             if (valid && code != 0)
                 atomicAdd(&heavy_count[pix], 1);
-            continue;
+            return;
         }
         bool hv = false;
         int entry = 0;
@@ -1082,6 +1096,16 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
         }
         warp_append(heavy, heavy_count, hv, entry);
     }
+}
+
+template <bool PROBE>
+__global__ void __launch_bounds__(kBlock, kLightBlocksPerSM)
+k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
+              int* __restrict__ heavy_count)
+{
+    __shared__ LightShared sh;
+    for (long long u = blockIdx.x; u < L.units; u += gridDim.x)
+        light_unit<PROBE>(P, L, u, num_queries, qcol, heavy, heavy_count, sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -1450,19 +1474,13 @@ __device__ bool coop_triangle(const RSample* in, int n, const Query& o, float di
     return false;
 }
 
-__global__ void __launch_bounds__(kCWarps * 32, TLFR_COOP_BLOCKS_PER_SM)
-k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ queue_count,
-             float4* __restrict__ qcol, int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap,
-             CoopScratch* __restrict__ scratch)
+// One warp: the queued output samples queue[b .. b+32) (of n) through the full
+// path, with the warp's working lists S and shared triangle-search bits T.
+__device__ __forceinline__ void coop_group(const QParams& P, const int* __restrict__ queue, int n, int b,
+                                           float4* __restrict__ qcol, int* __restrict__ ovf_queue,
+                                           int* __restrict__ ovf_count, int ovf_cap, CoopScratch& S, TriShared& T)
 {
-    __shared__ TriShared sh_tri[kCWarps];
     const int lane = threadIdx.x & 31;
-    const int warp = blockIdx.x * kCWarps + (threadIdx.x >> 5);
-    const int nwarps = gridDim.x * kCWarps;
-    CoopScratch& S = scratch[warp];
-    TriShared& T = sh_tri[threadIdx.x >> 5];
-    const int n = *queue_count;
-    for (int b = warp * 32; b < n; b += nwarps * 32)
     {
         // 1. per-lane traversal and leaf sort: at 2R for output samples the light
         // pass found to need it, at 1R for those that outgrew the light pass's
@@ -1663,6 +1681,19 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
     }
 }
 
+__global__ void __launch_bounds__(kCWarps * 32, TLFR_COOP_BLOCKS_PER_SM)
+k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ queue_count,
+             float4* __restrict__ qcol, int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap,
+             CoopScratch* __restrict__ scratch)
+{
+    __shared__ TriShared sh_tri[kCWarps];
+    const int warp = blockIdx.x * kCWarps + (threadIdx.x >> 5);
+    const int nwarps = gridDim.x * kCWarps;
+    const int n = *queue_count;
+    for (int b = warp * 32; b < n; b += nwarps * 32)
+        coop_group(P, queue, n, b, qcol, ovf_queue, ovf_count, ovf_cap, scratch[warp], sh_tri[threadIdx.x >> 5]);
+}
+
 // Statistics pass: every output sample through the full path with the
 // reference's counters (TreeGather::Stats).
 __global__ void __launch_bounds__(kBlock)
@@ -1820,10 +1851,11 @@ size_t coop_scratch_bytes(int num_sms) { return sizeof(CoopScratch) * (size_t)nu
 
 // light pass iterations and lane map of a frame (nq_probe > 0: the router's
 // probe pass over nq_probe output samples, linear)
-static LightMap light_map(const Ctx& c, long long nq_probe = 0)
+static LightMap light_map(const Ctx& c, long long nq_probe = 0, int shape = kDefaultShape)
 {
     LightMap L{};
-    if (nq_probe > 0 || c.out_spp % kTileSamples != 0)
+    const int tw = kTileShapes[shape][0], th = kTileShapes[shape][1], sw = 32 / (tw * th);
+    if (nq_probe > 0 || c.out_spp % (4 * sw) != 0)
     {
         const long long nq = nq_probe > 0 ? nq_probe : (long long)c.W * c.H * c.out_spp;
         L.mode = kMapLinear;
@@ -1831,9 +1863,10 @@ static LightMap light_map(const Ctx& c, long long nq_probe = 0)
         return L;
     }
     L.mode = kMapTiles;
-    L.tiles_x = (c.W + kTileW - 1) / kTileW;
-    L.groups = c.out_spp / kTileSamples;
-    L.units = (long long)L.tiles_x * ((c.H + kTileH - 1) / kTileH) * L.groups;
+    L.tw = tw; L.th = th; L.sw = sw;
+    L.tiles_x = (c.W + tw - 1) / tw;
+    L.groups = c.out_spp / (4 * sw);
+    L.units = (long long)L.tiles_x * ((c.H + th - 1) / th) * L.groups;
     return L;
 }
 size_t overflow_scratch_bytes() { return slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf) * kOvSlots; }
@@ -1857,133 +1890,495 @@ tlfr_status route_probe(Ctx& c, int* d_counts)
     return TLFR_OK;
 }
 
-// Every buffer a frame's reconstruction uses, allocated ahead (a captured
-// frame may not allocate).
-tlfr_status frame_prepare(Ctx& c, bool own_scratch)
-{
-    const long long npix = (long long)c.W * c.H;
-    const long long nq = npix * c.out_spp;
-    if (nq >= kQueueRestart)
-    {
-        c.error = "more than 2^30 output samples in one frame";
-        return TLFR_BAD_ARG;
-    }
-    if ((size_t)nq > c.qcol_cap)
-    {
-        cudaFree(c.qcol); cudaFree(c.heavy_queue); cudaFree(c.ovf_queue);
-        c.qcol = nullptr; c.heavy_queue = nullptr; c.ovf_queue = nullptr; c.qcol_cap = 0; c.ovf_cap = 0;
-        CKQ(cudaMalloc(&c.qcol, sizeof(float4) * nq));
-        CKQ(cudaMalloc(&c.heavy_queue, sizeof(int) * nq));
-        CKQ(cudaMalloc(&c.ovf_queue, sizeof(int) * nq));
-        c.qcol_cap = (size_t)nq;
-        c.ovf_cap = (size_t)nq;
-    }
-    if (!c.d_stats)
-        CKQ(cudaMalloc(&c.d_stats, sizeof(DevStats) + 8 * sizeof(int)));
-    if (own_scratch && !c.coop_scratch)
-    {
-        c.coop_scratch_bytes = coop_scratch_bytes(c.num_sms);
-        CKQ(cudaMalloc(&c.coop_scratch, c.coop_scratch_bytes));
-    }
-    if (own_scratch && !c.ovf_scratch)
-    {
-        c.ovf_scratch_bytes = overflow_scratch_bytes();
-        CKQ(cudaMalloc(&c.ovf_scratch, c.ovf_scratch_bytes));
-    }
-    if (c.router && !c.route_prob)
-    {
-        CKQ(cudaMalloc(&c.route_feats, sizeof(float) * kRouteFeatures * npix));
-        CKQ(cudaMalloc(&c.route_prob, sizeof(float) * npix));
-        CKQ(cudaMalloc(&c.route_fast, npix));
-    }
-    return TLFR_OK;
-}
-
 int light_default_blocks(const Ctx& c)
 {
     const LightMap L = light_map(c);
     return (int)std::min<long long>(L.units, (long long)c.num_sms * 64);
 }
 
-// One frame's reconstruction issued on stream s with no host synchronisation:
-// router (when set), light pass on light_blocks blocks, cooperative pass,
-// large-capacity pass (its count read on the device), pixel resolve.  Requires
-// frame_prepare() and, with a router, one earlier reconstruction (the router's
-// feature scratch).  Capacity failures are counted on the device
-// (frame_hard_failures).
-tlfr_status frame_enqueue(Ctx& c, float4* d_rgba, cudaStream_t s, int light_blocks, void* coop_scratch,
-                          void* ovf_scratch)
+// ---------------------------------------------------------------------------
+// Batches: many frames (contexts of any size and spp, or one context under
+// several output settings, each with its own output pattern) in one CUDA graph.
+// Each pass runs as ONE persistent launch over all frames of a chunk: blocks
+// (warps for the full path) take work items from a device counter, find their
+// frame by a binary search over the items' frame offsets and run that frame's
+// unit with its parameters from a device table of frame descriptors.  The
+// working storage (per-output-sample colours and queues) belongs to the batch;
+// frames are grouped into chunks whose storage fits the budget, and the chunks
+// run one after another in the graph, reusing it.  The light pass's tile shape
+// is chosen per frame by timing each shape (autotune).
+// ---------------------------------------------------------------------------
+struct FrameDesc
 {
-    if (!coop_scratch)
-        coop_scratch = c.coop_scratch;
-    if (!ovf_scratch)
-        ovf_scratch = c.ovf_scratch;
-    const long long npix = (long long)c.W * c.H;
-    const long long nq = npix * c.out_spp;
-    int* counters = reinterpret_cast<int*>(c.d_stats + 1);
-    QParams P = make_params(c);
-    cudaStream_t saved = c.stream;
-    c.stream = s;
-    CKQ(cudaMemsetAsync(c.d_stats, 0, sizeof(DevStats) + 8 * sizeof(int), s));
-    if (c.router)
+    QParams P;
+    LightMap L;
+    long long nq;
+    long long npix;
+    float4* qcol;
+    int* heavy;
+    int* ovf;
+    int* counters;          // [0] overflow queue, [1] capacity failures, [2] heavy queue
+    float4* out;
+};
+
+namespace
+{
+
+// frame of global index x: the last f with begin[f] <= x
+__device__ __forceinline__ int frame_of(const long long* __restrict__ begin, int n, long long x)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
     {
-        std::string err;
-        tlfr_status rs = route_features(c, c.route_feats, err);
-        if (rs == TLFR_OK)
-            rs = route_predict(*c.router, c.route_feats, npix, c.route_prob, s, err);
-        if (rs == TLFR_OK)
-            rs = route_flags(c, c.route_prob, c.route_hi, c.route_fast, err);
-        if (rs != TLFR_OK)
-        {
-            c.stream = saved;
-            c.error = err;
-            return rs;
-        }
-        c.launches++;
-        P.route_fast = c.route_fast;
+        const int mid = (lo + hi + 1) >> 1;
+        if (begin[mid] <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
     }
-    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
-                counters + 2);
-    TLFR_LAUNCH(c, k_query_coop, coop_blocks(c), kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol, c.ovf_queue,
-                counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(coop_scratch));
-    TLFR_LAUNCH(c, k_query_overflow, kOvSlots / 64, 64, s, P, c.ovf_queue, counters + 0, (int)c.ovf_cap, c.qcol,
-                (char*)ovf_scratch, slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf), kOvSlots, kOvStack, kOvLeaf,
-                kOvRs, kOvSurf, counters + 1, c.d_stats, 0);
-    TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, (long long)c.num_sms * 32), 128, s, c.qcol,
-                c.out_spp, d_rgba, npix);
-    c.stream = saved;
-    CKQ(cudaGetLastError());
-    return TLFR_OK;
+    return lo;
 }
 
-// Output samples of the last enqueued frame that exceeded every capacity.
-tlfr_status frame_hard_failures(Ctx& c, cudaStream_t s, int* hard)
+// Light pass over every frame of a chunk: a block takes one unit at a time.
+__global__ void __launch_bounds__(kBlock, kLightBlocksPerSM)
+k_batch_light(const FrameDesc* __restrict__ fd, const long long* __restrict__ unit_begin, int nframes,
+              unsigned long long* __restrict__ next_unit)
 {
-    int* counters = reinterpret_cast<int*>(c.d_stats + 1);
-    CKQ(cudaMemcpyAsync(hard, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CKQ(cudaStreamSynchronize(s));
-    return TLFR_OK;
+    __shared__ LightShared sh;
+    __shared__ QParams sP;
+    __shared__ LightMap sL;
+    __shared__ long long sU;
+    __shared__ int sF;
+    const long long total = unit_begin[nframes];
+    int cur = -1;
+    for (;;)
+    {
+        if (threadIdx.x == 0)
+        {
+            const long long u = (long long)atomicAdd(next_unit, 1ull);
+            sU = u;
+            sF = u < total ? frame_of(unit_begin, nframes, u) : -1;
+            if (sF >= 0 && sF != cur)
+            {
+                sP = fd[sF].P;
+                sL = fd[sF].L;
+            }
+        }
+        __syncthreads();
+        const long long u = sU;
+        const int f = sF;
+        if (u >= total)
+            break;
+        cur = f;
+        const FrameDesc& D = fd[f];
+        light_unit<false>(sP, sL, u - unit_begin[f], D.nq, D.qcol, D.heavy, D.counters + 2, sh);
+        __syncthreads();
+    }
 }
 
-// Device time of the light pass alone with light_blocks blocks (autotuning).
-tlfr_status light_trial(Ctx& c, cudaStream_t s, int light_blocks, float* ms)
+// Work items of the full-path pass: 32 queued output samples each.
+__global__ void k_batch_items(const FrameDesc* __restrict__ fd, int nframes, long long* __restrict__ item_begin)
 {
-    const long long nq = (long long)c.W * c.H * c.out_spp;
-    int* counters = reinterpret_cast<int*>(c.d_stats + 1);
-    QParams P = make_params(c);
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    long long acc = 0;
+    for (int f = 0; f < nframes; f++)
+    {
+        item_begin[f] = acc;
+        acc += (fd[f].counters[2] + 31) / 32;
+    }
+    item_begin[nframes] = acc;
+}
+
+// Full-path pass over every frame of a chunk: a warp takes one item at a time.
+__global__ void __launch_bounds__(kCWarps * 32, TLFR_COOP_BLOCKS_PER_SM)
+k_batch_coop(const FrameDesc* __restrict__ fd, const long long* __restrict__ item_begin, int nframes,
+             unsigned long long* __restrict__ next_item, CoopScratch* __restrict__ scratch)
+{
+    __shared__ TriShared sh_tri[kCWarps];
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.x * kCWarps + (threadIdx.x >> 5);
+    const long long total = item_begin[nframes];
+    for (;;)
+    {
+        long long it = 0;
+        if (lane == 0)
+            it = (long long)atomicAdd(next_item, 1ull);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= total)
+            break;
+        const int f = frame_of(item_begin, nframes, it);
+        const FrameDesc& D = fd[f];
+        coop_group(D.P, D.heavy, D.counters[2], (int)(it - item_begin[f]) * 32, D.qcol, D.ovf, D.counters + 0,
+                   (int)D.nq, scratch[warp], sh_tri[threadIdx.x >> 5]);
+    }
+}
+
+// Pixels of every frame of a chunk (k_resolve per frame).
+__global__ void k_batch_resolve(const FrameDesc* __restrict__ fd, const long long* __restrict__ pix_begin, int nframes)
+{
+    const long long total = pix_begin[nframes];
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x)
+    {
+        const int f = frame_of(pix_begin, nframes, g);
+        const FrameDesc& D = fd[f];
+        const long long p = g - pix_begin[f];
+        const int M = D.P.M;
+        const float4* c = D.qcol + p * M;
+        float4 s = make_float4(0, 0, 0, 0);
+        for (int i = 0; i < M; i++)
+        {
+            const float4 v = c[i];
+            s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+        }
+        if (s.w == 0)
+            s = make_float4(1, 0, 0, 1);
+        const float r = rcp(s.w);
+        D.out[p] = make_float4(s.x * r, s.y * r, s.z * r, s.w * r);
+    }
+}
+
+} // namespace
+
+struct BatchChunk
+{
+    int first = 0, count = 0;           // frames [first, first + count)
+    FrameDesc* d_desc = nullptr;        // into BatchPlan::d_desc
+    long long* d_unit_begin = nullptr;  // count + 1
+    long long* d_item_begin = nullptr;  // count + 1
+    long long* d_pix_begin = nullptr;   // count + 1
+    unsigned long long* d_work = nullptr;   // [0] next light unit, [1] next full-path item
+};
+
+struct BatchPlan
+{
+    std::vector<BatchEntry> entries;
+    std::vector<FrameDesc> desc;        // host copy
+    std::vector<BatchChunk> chunks;
+    std::vector<int> shape;             // tile shape per frame
+    std::vector<float*> patterns;       // per frame: its own output pattern (or null)
+    FrameDesc* d_desc = nullptr;
+    long long* d_offsets = nullptr;
+    unsigned long long* d_work = nullptr;
+    int* d_counters = nullptr;          // 4 per frame
+    float4* qcol = nullptr;
+    int* heavy = nullptr;
+    int* ovf = nullptr;
+    void* coop_scratch = nullptr;
+    void* ovf_scratch = nullptr;
+    int num_sms = 0;
+};
+
+size_t batch_storage_bytes(long long nq) { return (size_t)nq * (sizeof(float4) + 2 * sizeof(int)); }
+
+void batch_release(BatchPlan& bp)
+{
+    for (float* p : bp.patterns)
+        if (p) cudaFree(p);
+    void* ptrs[] = { bp.d_desc, bp.d_offsets, bp.d_work, bp.d_counters, bp.qcol, bp.heavy, bp.ovf, bp.coop_scratch,
+                     bp.ovf_scratch };
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    bp = BatchPlan{};
+}
+
+#define CKB(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { err = std::string(#x) + ": " + cudaGetErrorString(_e); return (_e == cudaErrorMemoryAllocation) ? TLFR_OOM : TLFR_CUDA; } } while (0)
+
+// The light pass of one frame alone with a given tile shape (autotune), over
+// its first eighth of block iterations (the top rows of the frame's tiles).
+static tlfr_status light_trial(const FrameDesc& D, const Ctx& c, int shape, cudaStream_t s, float* ms,
+                               std::string& err)
+{
     cudaEvent_t e0, e1;
-    CKQ(cudaEventCreate(&e0));
-    CKQ(cudaEventCreate(&e1));
-    CKQ(cudaMemsetAsync(counters, 0, 8 * sizeof(int), s));
-    CKQ(cudaEventRecord(e0, s));
-    TLFR_LAUNCH(c, k_query_light<false>, light_blocks, kBlock, s, P, light_map(c), nq, c.qcol, c.heavy_queue,
-                counters + 2);
-    CKQ(cudaEventRecord(e1, s));
-    CKQ(cudaEventSynchronize(e1));
-    CKQ(cudaEventElapsedTime(ms, e0, e1));
+    CKB(cudaEventCreate(&e0));
+    CKB(cudaEventCreate(&e1));
+    LightMap L = D.L;
+    {
+        // the shape's map for this frame's output samples
+        Ctx tmp;
+        tmp.W = c.W; tmp.H = c.H; tmp.out_spp = D.P.M;
+        L = light_map(tmp, 0, shape);
+        L.units = std::max<long long>(std::min<long long>(L.units, 4096), L.units / 8);
+    }
+    const int blocks = (int)std::min<long long>(L.units, (long long)c.num_sms * 64);
+    CKB(cudaMemsetAsync(D.counters, 0, 4 * sizeof(int), s));
+    CKB(cudaEventRecord(e0, s));
+    k_query_light<false><<<blocks, kBlock, 0, s>>>(D.P, L, D.nq, D.qcol, D.heavy, D.counters + 2);
+    CKB(cudaEventRecord(e1, s));
+    CKB(cudaEventSynchronize(e1));
+    CKB(cudaEventElapsedTime(ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    CKQ(cudaGetLastError());
+    CKB(cudaGetLastError());
+    return TLFR_OK;
+}
+
+tlfr_status batch_build(BatchPlan& bp, const std::vector<BatchEntry>& entries, cudaStream_t s, bool autotune,
+                        size_t budget, std::string& err)
+{
+    const int n = (int)entries.size();
+    bp.entries = entries;
+    bp.num_sms = entries[0].ctx->num_sms;
+    bp.desc.resize(n);
+    bp.shape.assign(n, kDefaultShape);
+    bp.patterns.assign(n, nullptr);
+    // per frame: output pattern, parameters, sizes
+    std::vector<long long> nq(n), npix(n);
+    for (int f = 0; f < n; f++)
+    {
+        Ctx& c = *entries[f].ctx;
+        FrameDesc& D = bp.desc[f];
+        D.P = make_params(c);
+        if (entries[f].output)
+        {
+            const tlfr_params& o = *entries[f].output;
+            const bool ov = o.override_uvt != 0;
+            const int M = o.output_spp > 0 ? o.output_spp : (ov ? 1 : 128);
+            if (M > 1024)
+            {
+                err = "frame " + std::to_string(f) + ": output_spp out of range";
+                return TLFR_BAD_ARG;
+            }
+            std::vector<float> pat;
+            generate_output_pattern(M, ov, o.uvt, pat);
+            CKB(cudaMalloc(&bp.patterns[f], sizeof(float) * pat.size()));
+            CKB(cudaMemcpy(bp.patterns[f], pat.data(), sizeof(float) * pat.size(), cudaMemcpyHostToDevice));
+            D.P.pattern = bp.patterns[f];
+            D.P.M = M;
+            D.P.lens_filter = o.lens_filter;
+            D.P.time_filter = o.time_filter;
+        }
+        npix[f] = (long long)c.W * c.H;
+        nq[f] = npix[f] * D.P.M;
+        if (nq[f] >= kQueueRestart)
+        {
+            err = "frame " + std::to_string(f) + ": more than 2^30 output samples";
+            return TLFR_BAD_ARG;
+        }
+        D.nq = nq[f];
+        D.npix = npix[f];
+        D.out = entries[f].out;
+        Ctx tmp;
+        tmp.W = c.W; tmp.H = c.H; tmp.out_spp = D.P.M;
+        D.L = light_map(tmp, 0, kDefaultShape);
+    }
+    // chunks: consecutive frames whose storage fits the budget (a frame larger
+    // than the budget is a chunk of its own)
+    size_t largest = 0;
+    for (int f = 0; f < n;)
+    {
+        BatchChunk ch;
+        ch.first = f;
+        size_t bytes = 0;
+        while (f < n && (ch.count == 0 || bytes + batch_storage_bytes(nq[f]) <= budget))
+        {
+            bytes += batch_storage_bytes(nq[f]);
+            f++;
+            ch.count++;
+        }
+        largest = std::max(largest, bytes);
+        bp.chunks.push_back(ch);
+    }
+    long long cap = 0;
+    for (const BatchChunk& ch : bp.chunks)
+    {
+        long long t = 0;
+        for (int f = ch.first; f < ch.first + ch.count; f++)
+            t += nq[f];
+        cap = std::max(cap, t);
+    }
+    CKB(cudaMalloc(&bp.qcol, sizeof(float4) * cap));
+    CKB(cudaMalloc(&bp.heavy, sizeof(int) * cap));
+    CKB(cudaMalloc(&bp.ovf, sizeof(int) * cap));
+    CKB(cudaMalloc(&bp.d_counters, sizeof(int) * 4 * n));
+    CKB(cudaMalloc(&bp.coop_scratch, coop_scratch_bytes(bp.num_sms)));
+    CKB(cudaMalloc(&bp.ovf_scratch, overflow_scratch_bytes()));
+    for (const BatchChunk& ch : bp.chunks)
+    {
+        long long off = 0;
+        for (int f = ch.first; f < ch.first + ch.count; f++)
+        {
+            FrameDesc& D = bp.desc[f];
+            D.qcol = bp.qcol + off;
+            D.heavy = bp.heavy + off;
+            D.ovf = bp.ovf + off;
+            D.counters = bp.d_counters + 4 * f;
+            off += nq[f];
+        }
+    }
+    // router flags of frames with a router (and their context's own pattern)
+    for (int f = 0; f < n; f++)
+    {
+        Ctx& c = *entries[f].ctx;
+        if (c.router && !entries[f].output && !c.route_prob)
+        {
+            CKB(cudaMalloc(&c.route_feats, sizeof(float) * kRouteFeatures * npix[f]));
+            CKB(cudaMalloc(&c.route_prob, sizeof(float) * npix[f]));
+            CKB(cudaMalloc(&c.route_fast, npix[f]));
+        }
+        if (c.router && !entries[f].output)
+            bp.desc[f].P.route_fast = c.route_fast;
+    }
+    // autotune: each frame's light pass alone with every tile shape, once per
+    // frame class (size, input spp, output samples per pixel)
+    if (autotune)
+    {
+        std::vector<std::array<int, 5>> seen;    // (W, H, spp, M, shape)
+        for (int f = 0; f < n; f++)
+        {
+            const Ctx& cf = *entries[f].ctx;
+            bool known = false;
+            for (const auto& k : seen)
+                if (k[0] == cf.W && k[1] == cf.H && k[2] == cf.spp_in && k[3] == bp.desc[f].P.M)
+                {
+                    bp.shape[f] = k[4];
+                    known = true;
+                }
+            float best = known ? -1.0f : 1e30f;
+            for (int sh = 0; sh < (int)(sizeof(kTileShapes) / sizeof(kTileShapes[0])); sh++)
+            {
+                if (known)
+                    break;
+                float ms = 0;
+                const tlfr_status st = light_trial(bp.desc[f], *entries[f].ctx, sh, s, &ms, err);
+                if (st != TLFR_OK)
+                    return st;
+                if (ms < best)
+                {
+                    best = ms;
+                    bp.shape[f] = sh;
+                }
+            }
+            if (!known)
+                seen.push_back({ cf.W, cf.H, cf.spp_in, bp.desc[f].P.M, bp.shape[f] });
+            Ctx tmp;
+            tmp.W = entries[f].ctx->W; tmp.H = entries[f].ctx->H; tmp.out_spp = bp.desc[f].P.M;
+            bp.desc[f].L = light_map(tmp, 0, bp.shape[f]);
+        }
+    }
+    // device tables
+    CKB(cudaMalloc(&bp.d_desc, sizeof(FrameDesc) * n));
+    CKB(cudaMalloc(&bp.d_offsets, sizeof(long long) * 3 * (n + bp.chunks.size())));
+    CKB(cudaMalloc(&bp.d_work, sizeof(unsigned long long) * 2 * bp.chunks.size()));
+    std::vector<long long> offs;
+    offs.reserve(3 * (n + bp.chunks.size()));
+    for (size_t k = 0; k < bp.chunks.size(); k++)
+    {
+        BatchChunk& ch = bp.chunks[k];
+        ch.d_desc = bp.d_desc + ch.first;
+        ch.d_work = bp.d_work + 2 * k;
+        const size_t base = offs.size();
+        long long u = 0, pxl = 0;
+        std::vector<long long> ub, pb;
+        for (int f = ch.first; f < ch.first + ch.count; f++)
+        {
+            ub.push_back(u);
+            pb.push_back(pxl);
+            u += bp.desc[f].L.units;
+            pxl += npix[f];
+        }
+        ub.push_back(u);
+        pb.push_back(pxl);
+        offs.insert(offs.end(), ub.begin(), ub.end());
+        offs.insert(offs.end(), pb.begin(), pb.end());
+        offs.insert(offs.end(), ch.count + 1, 0LL);      // item offsets, filled on the device
+        ch.d_unit_begin = bp.d_offsets + base;
+        ch.d_pix_begin = bp.d_offsets + base + ch.count + 1;
+        ch.d_item_begin = bp.d_offsets + base + 2 * (ch.count + 1);
+    }
+    CKB(cudaMemcpy(bp.d_offsets, offs.data(), sizeof(long long) * offs.size(), cudaMemcpyHostToDevice));
+    CKB(cudaMemcpy(bp.d_desc, bp.desc.data(), sizeof(FrameDesc) * n, cudaMemcpyHostToDevice));
+    return TLFR_OK;
+}
+
+// Every pass of every chunk, on stream s, with no host synchronisation (the
+// counts the full-path and large-capacity passes need are read on the device).
+tlfr_status batch_enqueue(BatchPlan& bp, cudaStream_t s, std::string& err, long long* launches)
+{
+    const int n = (int)bp.entries.size();
+    long long L = 0;
+    CKB(cudaMemsetAsync(bp.d_counters, 0, sizeof(int) * 4 * n, s));
+    CKB(cudaMemsetAsync(bp.d_work, 0, sizeof(unsigned long long) * 2 * bp.chunks.size(), s));
+    for (const BatchChunk& ch : bp.chunks)
+    {
+        // the router's flags for this chunk's routed frames (their descriptors
+        // point at the context's flags)
+        for (int f = ch.first; f < ch.first + ch.count; f++)
+        {
+            Ctx& c = *bp.entries[f].ctx;
+            if (!c.router || bp.entries[f].output)
+                continue;
+            cudaStream_t saved = c.stream;
+            c.stream = s;
+            const long long np = (long long)c.W * c.H;
+            tlfr_status rs = route_features(c, c.route_feats, err);
+            if (rs == TLFR_OK)
+                rs = route_predict(*c.router, c.route_feats, np, c.route_prob, s, err);
+            if (rs == TLFR_OK)
+                rs = route_flags(c, c.route_prob, c.route_hi, c.route_fast, err);
+            c.stream = saved;
+            if (rs != TLFR_OK)
+                return rs;
+            L += 7;
+        }
+        const int lb = bp.num_sms * kLightBlocksPerSM;
+        k_batch_light<<<lb, kBlock, 0, s>>>(ch.d_desc, ch.d_unit_begin, ch.count, ch.d_work + 0);
+        k_batch_items<<<1, 32, 0, s>>>(ch.d_desc, ch.count, ch.d_item_begin);
+        k_batch_coop<<<bp.num_sms * kCoopBlocksPerSM, kCWarps * 32, 0, s>>>(ch.d_desc, ch.d_item_begin, ch.count,
+                                                                           ch.d_work + 1,
+                                                                           reinterpret_cast<CoopScratch*>(bp.coop_scratch));
+        L += 3;
+        for (int f = ch.first; f < ch.first + ch.count; f++)
+        {
+            const FrameDesc& D = bp.desc[f];
+            k_query_overflow<<<kOvSlots / 64, 64, 0, s>>>(D.P, D.ovf, D.counters + 0, (int)D.nq, D.qcol,
+                                                         (char*)bp.ovf_scratch,
+                                                         slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf), kOvSlots,
+                                                         kOvStack, kOvLeaf, kOvRs, kOvSurf, D.counters + 1, nullptr, 0);
+            L++;
+        }
+        k_batch_resolve<<<bp.num_sms * 32, 128, 0, s>>>(ch.d_desc, ch.d_pix_begin, ch.count);
+        L++;
+    }
+    CKB(cudaGetLastError());
+    if (launches)
+        *launches = L;
+    return TLFR_OK;
+}
+
+BatchPlan* batch_plan_new() { return new (std::nothrow) BatchPlan(); }
+
+void batch_plan_delete(BatchPlan* bp)
+{
+    if (bp)
+    {
+        batch_release(*bp);
+        delete bp;
+    }
+}
+
+// tile shape (index into kTileShapes) per frame, chunk per frame
+void batch_info(const BatchPlan& bp, int* shapes, int* chunks)
+{
+    for (size_t f = 0; f < bp.entries.size(); f++)
+        if (shapes)
+            shapes[f] = bp.shape[f];
+    for (size_t k = 0; k < bp.chunks.size(); k++)
+        for (int f = bp.chunks[k].first; f < bp.chunks[k].first + bp.chunks[k].count; f++)
+            if (chunks)
+                chunks[f] = (int)k;
+}
+
+// Output samples that exceeded every capacity, over all frames of the last run.
+tlfr_status batch_failures(BatchPlan& bp, cudaStream_t s, std::vector<int>& hard, std::string& err)
+{
+    const int n = (int)bp.entries.size();
+    std::vector<int> cnt(4 * n);
+    CKB(cudaMemcpyAsync(cnt.data(), bp.d_counters, sizeof(int) * 4 * n, cudaMemcpyDeviceToHost, s));
+    CKB(cudaStreamSynchronize(s));
+    hard.resize(n);
+    for (int f = 0; f < n; f++)
+        hard[f] = cnt[4 * f + 1] + (cnt[4 * f + 0] > (int)bp.desc[f].nq ? 1 : 0);
     return TLFR_OK;
 }
 

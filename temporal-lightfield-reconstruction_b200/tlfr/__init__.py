@@ -129,6 +129,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_batch_run": (ctypes.c_int, [_VP]),
         "tlfr_batch_sync": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double)]),
         "tlfr_batch_info": (ctypes.c_int, [_VP, _IP]),
+        "tlfr_batch_layout": (ctypes.c_int, [_VP, _IP, ctypes.POINTER(ctypes.c_longlong)]),
+        "tlfr_batch_create_frames": (ctypes.c_int, [_VP, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_size_t,
+                                                    ctypes.POINTER(_VP)]),
         "tlfr_batch_last_error": (ctypes.c_char_p, [_VP]),
         "tlfr_batch_destroy": (None, [_VP]),
     }
@@ -450,17 +453,34 @@ class Router:
         self.close()
 
 
-class Batch:
-    """Several built TreeGather contexts reconstructed as one CUDA graph (tlfr_batch_*)."""
+class _BatchFrame(ctypes.Structure):
+    _fields_ = [("ctx", _VP), ("output", ctypes.POINTER(_Params)), ("d_rgba", _VP)]
 
-    def __init__(self, trees: Sequence["TreeGather"], outputs: Sequence[int], stream: int = 0, autotune: bool = True):
+
+TILE_SHAPES = ["4x2 px x 4 samples", "8x4 px x 1 sample", "4x4 px x 2 samples", "2x2 px x 8 samples",
+               "2x1 px x 16 samples"]
+
+
+class Batch:
+    """Frames reconstructed together as one CUDA graph (tlfr_batch_*): built
+    TreeGather contexts, each with its own output settings or with an output
+    setting of the frame's own (a sweep over one hierarchy: pass the same tree
+    with different CameraParams)."""
+
+    def __init__(self, trees: Sequence["TreeGather"], outputs: Sequence[int], stream: int = 0, autotune: bool = True,
+                 params: Optional[Sequence[Optional["CameraParams"]]] = None, budget_bytes: int = 0):
         lib = load_library()
         n = len(trees)
         self._trees = list(trees)
-        hs = (_VP * n)(*[t.handle for t in trees])
-        outs = (_VP * n)(*[_VP(p) for p in outputs])
+        self._params = [p._to_c(1.0, 1.0) if p is not None else None for p in (params or [None] * n)]
+        frames = (_BatchFrame * n)()
+        for i in range(n):
+            frames[i].ctx = trees[i].handle
+            frames[i].output = ctypes.pointer(self._params[i]) if self._params[i] is not None else None
+            frames[i].d_rgba = _VP(outputs[i])
         h = _VP()
-        st = lib.tlfr_batch_create(hs, n, outs, _VP(stream), 1 if autotune else 0, ctypes.byref(h))
+        st = lib.tlfr_batch_create_frames(frames, n, _VP(stream), 1 if autotune else 0, ctypes.c_size_t(budget_bytes),
+                                          ctypes.byref(h))
         if st != 0:
             raise TlfrError(st, (lib.tlfr_batch_last_error(None) or b"").decode())
         self._h = h
@@ -478,10 +498,18 @@ class Batch:
         self._ok(load_library().tlfr_batch_sync(self._h, ctypes.byref(ms)))
         return ms.value
 
-    def light_blocks(self):
+    def tile_shapes(self):
+        """The light-pass tile shape chosen per frame (index into TILE_SHAPES)."""
         b = np.zeros(self.n, np.int32)
         self._ok(load_library().tlfr_batch_info(self._h, _i32p(b)))
         return b
+
+    def layout(self):
+        """(chunk of each frame, kernel launches of one run)."""
+        c = np.zeros(self.n, np.int32)
+        nl = ctypes.c_longlong()
+        self._ok(load_library().tlfr_batch_layout(self._h, _i32p(c), ctypes.byref(nl)))
+        return c, nl.value
 
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:
