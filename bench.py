@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--route-threshold", type=float, default=0.8)
     ap.add_argument("--route-labels", default="gt", choices=["gt", "plain"],
                     help="router labels against the scene's ground truth or the plain image")
-    ap.add_argument("--route-tol", type=float, default=2e-5,
+    ap.add_argument("--route-tol", type=float, default=0.0,
                     help="label tolerance: squared RGB error above the plain pixel's (gt) or channel difference")
     ap.add_argument("--gt-samples", type=int, default=1024, help="ground-truth samples per pixel")
     ap.add_argument("--batch-frames", type=int, default=48, help="uneven-buffer batch size (0: no batch run)")
@@ -288,7 +288,7 @@ def train_router(args, device, W, H, S):
     return router, info
 
 
-def routing_eval(args, device, router, W, H, S):
+def routing_eval(args, device, router, W, H, S, thresholds=None):
     """The router on held-out frames (seeds 200, 201, ...): per seed the plain
     method, the routed form and every pixel on the fast path (no network), each
     timed over full steps (hierarchy build + reconstruction, CUDA events), and
@@ -298,6 +298,7 @@ def routing_eval(args, device, router, W, H, S):
     import tlfr
     stream = torch.cuda.current_stream()
     rows = []
+    thresholds = sorted(set(thresholds or [args.route_threshold, 0.5]))
     for seed in range(200, 200 + args.route_eval):
         rec, coc = tlfr.synth_scene(PRESET, W, H, S, seed)
         d = torch.from_numpy(rec).cuda()
@@ -322,36 +323,48 @@ def routing_eval(args, device, router, W, H, S):
             return statistics.median(ms), out.cpu().numpy()
 
         ms_plain, plain = timed(None, 0.8)
-        ms_routed, routed = timed(router, args.route_threshold)
         ms_all, allfast = timed(router, 0.0)
         feats = torch.empty((H * W, 8), dtype=torch.float32, device="cuda")
         prob = torch.empty(H * W, dtype=torch.float32, device="cuda")
         g.route_features(feats.data_ptr())
         router.predict(feats.data_ptr(), W * H, prob.data_ptr())
-        frac = float((prob > args.route_threshold).float().mean().item())
+        gt = tlfr.synth_reference_image(PRESET, W, H, args.gt_samples, seed)
+        p_plain, p_all = psnr(plain, gt), psnr(allfast, gt)
+        row = {"seed": seed, "plain_ms": ms_plain, "all_fast_ms": ms_all, "psnr_plain_db": p_plain,
+               "psnr_all_fast_db": p_all, "psnr_loss_all_fast_db": p_plain - p_all, "thresholds": {}}
+        for thr in thresholds:
+            ms_r, routed = timed(router, thr)
+            p_r = psnr(routed, gt)
+            row["thresholds"][str(thr)] = {
+                "routed_ms": ms_r, "speedup": ms_plain / ms_r,
+                "fast_pixel_fraction": float((prob > thr).float().mean().item()),
+                "psnr_routed_db": p_r, "psnr_loss_db": p_plain - p_r,
+                "max_abs_err_vs_plain": float(np.abs(routed[..., :3] - plain[..., :3]).max()),
+                "psnr_routed_vs_plain_db": psnr(routed, plain)}
         g.set_routing(None)
         g.close()
         del d
-        gt = tlfr.synth_reference_image(PRESET, W, H, args.gt_samples, seed)
-        p_plain, p_routed, p_all = psnr(plain, gt), psnr(routed, gt), psnr(allfast, gt)
-        rows.append({
-            "seed": seed, "plain_ms": ms_plain, "routed_ms": ms_routed, "all_fast_ms": ms_all,
-            "speedup": ms_plain / ms_routed, "fast_pixel_fraction": frac,
-            "psnr_plain_db": p_plain, "psnr_routed_db": p_routed, "psnr_all_fast_db": p_all,
-            "psnr_loss_db": p_plain - p_routed, "psnr_loss_all_fast_db": p_plain - p_all,
-            "max_abs_err_vs_plain": float(np.abs(routed[..., :3] - plain[..., :3]).max()),
-            "psnr_routed_vs_plain_db": psnr(routed, plain),
-        })
-    med = lambda k: statistics.median(r[k] for r in rows)
+        rows.append(row)
+    med = lambda f: statistics.median(f(r) for r in rows)
+    summary = {}
+    for thr in thresholds:
+        k = str(thr)
+        summary[k] = {
+            "speedup_median": med(lambda r: r["thresholds"][k]["speedup"]),
+            "psnr_loss_db_max": max(r["thresholds"][k]["psnr_loss_db"] for r in rows),
+            "psnr_loss_db_median": med(lambda r: r["thresholds"][k]["psnr_loss_db"]),
+            "fast_pixel_fraction_median": med(lambda r: r["thresholds"][k]["fast_pixel_fraction"]),
+            "value": (W * H / (med(lambda r: r["thresholds"][k]["routed_ms"]) / 1e3)) / 1e6, "unit": "Mpix/s"}
+    main = summary[str(args.route_threshold)]
     return {
-        "seeds": [r["seed"] for r in rows], "per_seed": rows,
-        "speedup_median": med("speedup"), "speedup_all_fast_median": statistics.median(
-            r["plain_ms"] / r["all_fast_ms"] for r in rows),
-        "psnr_loss_db_max": max(r["psnr_loss_db"] for r in rows), "psnr_loss_db_median": med("psnr_loss_db"),
-        "psnr_loss_all_fast_db_median": med("psnr_loss_all_fast_db"),
-        "fast_pixel_fraction_median": med("fast_pixel_fraction"),
-        "value": (W * H / (med("routed_ms") / 1e3)) / 1e6, "unit": "Mpix/s",
-        "threshold": args.route_threshold, "gt_samples_per_pixel": args.gt_samples,
+        "seeds": [r["seed"] for r in rows], "per_seed": rows, "threshold": args.route_threshold,
+        "value": main["value"], "unit": "Mpix/s", "speedup_median": main["speedup_median"],
+        "psnr_loss_db_max": main["psnr_loss_db_max"], "psnr_loss_db_median": main["psnr_loss_db_median"],
+        "fast_pixel_fraction_median": main["fast_pixel_fraction_median"], "by_threshold": summary,
+        "no_network": {"plain_value": (W * H / (med(lambda r: r["plain_ms"]) / 1e3)) / 1e6,
+                       "all_fast_speedup_median": med(lambda r: r["plain_ms"] / r["all_fast_ms"]),
+                       "all_fast_psnr_loss_db_median": med(lambda r: r["psnr_loss_all_fast_db"])},
+        "psnr_plain_db_median": med(lambda r: r["psnr_plain_db"]), "gt_samples_per_pixel": args.gt_samples,
         "timing": "median of 2 full steps (hierarchy build + reconstruction) per seed after one warm-up, CUDA events",
     }
 
