@@ -400,6 +400,7 @@ def run_batch(args, device, router, steps, warmup):
         rec, coc = tlfr.synth_scene(tlfr.SCENE_CARDS, Wb, Hb, Sb, 1000 + k)
         d = torch.from_numpy(rec).cuda()
         g = tlfr.TreeGather(None, tlfr.CameraParams(device=device), device_records=(d.data_ptr(), (Wb, Hb, Sb), coc))
+        g.trim()
         if router is not None:
             g.set_routing(router, args.route_threshold)
         recs.append(d)

@@ -155,6 +155,11 @@ tlfr_status tlfr_reconstruct(tlfr_ctx* ctx, float* rgba, int rgba_on_device, tlf
  * existing context; the hierarchy is kept (App.cpp:616-694 refocus/animation loop). */
 tlfr_status tlfr_set_output(tlfr_ctx* ctx, const tlfr_params* params);
 
+/* Frees the hierarchy build's working storage of a built context (about 190
+ * bytes per input sample) and trims its node arrays to the nodes emitted; the
+ * hierarchy stays and reconstructions go on as before, a later rebuild
+ * allocates the storage again.  For many contexts held at once (batches).     */
+tlfr_status tlfr_trim(tlfr_ctx* ctx);
 tlfr_status tlfr_sync(tlfr_ctx* ctx);
 tlfr_status tlfr_get_stats(tlfr_ctx* ctx, tlfr_stats* stats);
 void        tlfr_destroy(tlfr_ctx* ctx);
@@ -306,9 +311,10 @@ tlfr_status tlfr_set_routing(tlfr_ctx* ctx, tlfr_router* router, float threshold
  * creation.  A frame's router (set on its context, own output settings only)
  * runs before its chunk.  Replaces the reference's per-frame reconstruct loops
  * of the animation and export paths (reconstruction_app/App.cpp:616-694,
- * a new TreeGather per (u,v) frame).  The graph holds the contexts' buffers as
- * they are at creation: after rebuilding a context with records of another
- * size, create the batch again.  The contexts (and routers) must outlive the
+ * a new TreeGather per (u,v) frame).  Creating a batch frees its contexts'
+ * hierarchy-build working storage (a later rebuild allocates it again), and
+ * the graph holds the contexts' buffers as they are at creation: after
+ * rebuilding a context, create the batch again.  The contexts (and routers) must outlive the
  * batch.  Outputs are device RGBA float images. */
 typedef struct tlfr_batch tlfr_batch;
 typedef struct tlfr_batch_frame

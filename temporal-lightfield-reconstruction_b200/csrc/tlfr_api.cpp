@@ -783,6 +783,15 @@ tlfr_status tlfr_set_output(tlfr_ctx* ctx, const tlfr_params* params)
     return upload_pattern(ctx);
 }
 
+tlfr_status tlfr_trim(tlfr_ctx* ctx)
+{
+    if (!ctx)
+        return fail(nullptr, TLFR_BAD_ARG, "tlfr_trim: null context");
+    cudaSetDevice(ctx->c.device);
+    const tlfr_status st = tlfr::release_build_scratch(ctx->c);
+    return st == TLFR_OK ? TLFR_OK : fail(ctx, st, "tlfr_trim: %s", ctx->c.error.c_str());
+}
+
 tlfr_status tlfr_sync(tlfr_ctx* ctx)
 {
     if (!ctx)
@@ -1248,6 +1257,23 @@ tlfr_status tlfr_batch_create_frames(const tlfr_batch_frame* frames, int n, void
         batch_free(b);
         return batch_fail(nullptr, TLFR_CUDA, m);
     };
+    std::string err;
+    tlfr_status st = TLFR_OK;
+    // the batch only queries its contexts: their build working storage goes
+    for (int i = 0; i < n && st == TLFR_OK; i++)
+    {
+        bool seen = false;
+        for (int j = 0; j < i; j++)
+            seen = seen || frames[j].ctx == frames[i].ctx;
+        if (!seen)
+            st = tlfr::release_build_scratch(frames[i].ctx->c);
+    }
+    if (st != TLFR_OK)
+    {
+        const std::string m = frames[0].ctx->c.error;
+        batch_free(b);
+        return batch_fail(nullptr, st, "tlfr_batch_create: " + m);
+    }
     if (budget_bytes == 0)
     {
         // default: half of the free device memory, at most 32 GiB
@@ -1255,8 +1281,7 @@ tlfr_status tlfr_batch_create_frames(const tlfr_batch_frame* frames, int n, void
         cudaMemGetInfo(&fr, &tot);
         budget_bytes = std::min<size_t>(fr / 2, (size_t)32 << 30);
     }
-    std::string err;
-    tlfr_status st = tlfr::batch_build(*b->plan, entries, b->stream, autotune != 0, budget_bytes, err);
+    st = tlfr::batch_build(*b->plan, entries, b->stream, autotune != 0, budget_bytes, err);
     if (st != TLFR_OK)
     {
         batch_free(b);

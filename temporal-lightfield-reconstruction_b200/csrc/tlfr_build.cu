@@ -998,6 +998,46 @@ const char* cuda_error_string(cudaError_t e) { return cudaGetErrorString(e); }
 
 #define CK(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { c.error = std::string(#x) + ": " + cudaGetErrorString(_e); return (_e == cudaErrorMemoryAllocation) ? TLFR_OOM : TLFR_CUDA; } } while (0)
 
+// Frees the hierarchy build's working storage of a built context (reprojected
+// samples, grid buckets, kd split, per-sample scratch) and trims the node
+// arrays, allocated for the worst case of two nodes per sample, to the nodes
+// the build emitted.  The hierarchy and its samples stay; a later rebuild
+// allocates the working storage again.
+tlfr_status release_build_scratch(Ctx& c)
+{
+    void** scratch[] = { (void**)&c.rp_pos, (void**)&c.rp_mot, (void**)&c.rp_cell, (void**)&c.cell_count,
+                         (void**)&c.cell_start, (void**)&c.cell_items, (void**)&c.kd, (void**)&c.kd_leaves_ordered,
+                         (void**)&c.perm, (void**)&c.box, (void**)&c.sbounds, (void**)&c.surface, (void**)&c.pending,
+                         (void**)&c.top, (void**)&c.ordered_n, (void**)&c.ordered_prefmax, (void**)&c.leaf_task_rank };
+    CK(cudaStreamSynchronize(c.stream));
+    for (void** p : scratch)
+    {
+        if (*p)
+            cudaFree(*p);
+        *p = nullptr;
+    }
+    c.cell_cap = 0;
+    c.kd_cap = 0;
+    c.leaf_cap = 0;
+    if (c.nodes && c.num_nodes > 0 && (size_t)c.num_nodes < c.node_cap)
+    {
+        QNode* nodes = nullptr;
+        float2* tspan = nullptr;
+        CK(cudaMalloc(&nodes, sizeof(QNode) * c.num_nodes));
+        CK(cudaMalloc(&tspan, sizeof(float2) * c.num_nodes));
+        CK(cudaMemcpy(nodes, c.nodes, sizeof(QNode) * c.num_nodes, cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(tspan, c.node_tspan, sizeof(float2) * c.num_nodes, cudaMemcpyDeviceToDevice));
+        cudaFree(c.nodes);
+        cudaFree(c.node_tspan);
+        c.nodes = nodes;
+        c.node_tspan = tspan;
+        c.node_cap = c.num_nodes;
+    }
+    // the per-sample arrays are reallocated with the node arrays at the next build
+    c.samp_cap = 0;
+    return TLFR_OK;
+}
+
 tlfr_status build_hierarchy(Ctx& c, const float* d_records)
 {
     cudaStream_t s = c.stream;
@@ -1010,10 +1050,13 @@ tlfr_status build_hierarchy(Ctx& c, const float* d_records)
         CK(cudaMalloc(&c.rp_pos, sizeof(float4) * n));
         CK(cudaMalloc(&c.rp_mot, sizeof(float4) * n));
         CK(cudaMalloc(&c.rp_cell, sizeof(int) * n));
-        CK(cudaMalloc(&c.hits, sizeof(int) * (size_t)c.W * c.H));
-        CK(cudaMalloc(&c.d_grid, sizeof(GridInfo) + sizeof(GridAccum) + 64 * sizeof(int)));
-        CK(cudaMalloc(&c.kd_level, sizeof(int) * 2 * (kMaxKdLevels + 2)));
     }
+    if (!c.hits)
+        CK(cudaMalloc(&c.hits, sizeof(int) * (size_t)c.W * c.H));
+    if (!c.d_grid)
+        CK(cudaMalloc(&c.d_grid, sizeof(GridInfo) + sizeof(GridAccum) + 64 * sizeof(int)));
+    if (!c.kd_level)
+        CK(cudaMalloc(&c.kd_level, sizeof(int) * 2 * (kMaxKdLevels + 2)));
     GridAccum* acc = reinterpret_cast<GridAccum*>(reinterpret_cast<char*>(c.d_grid) + sizeof(GridInfo));
     int* counters = reinterpret_cast<int*>(acc + 1);    // [0] kd counter, [1] node counter, [2] invalid, [3] scan total
 

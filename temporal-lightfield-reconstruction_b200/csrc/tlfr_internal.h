@@ -229,6 +229,8 @@ tlfr_status route_flags(Ctx& c, const float* d_prob, float hi, unsigned char* d_
 
 // build: reprojection, bucketing, kd split, leaf construction, emitNodes, top.
 tlfr_status build_hierarchy(Ctx& c, const float* d_records);
+// frees the build's working storage and trims the node arrays of a built context
+tlfr_status release_build_scratch(Ctx& c);
 // query: all output samples of the frame into rgba (device pointer).
 tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats);
 // Batches (tlfr_query.cu): frames reconstructed together in one CUDA graph with

@@ -97,6 +97,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_reconstruct": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.POINTER(Stats)]),
         "tlfr_set_output": (ctypes.c_int, [_VP, ctypes.POINTER(_Params)]),
         "tlfr_sync": (ctypes.c_int, [_VP]),
+        "tlfr_trim": (ctypes.c_int, [_VP]),
         "tlfr_get_stats": (ctypes.c_int, [_VP, ctypes.POINTER(Stats)]),
         "tlfr_destroy": (None, [_VP]),
         "tlfr_last_error": (ctypes.c_char_p, [_VP]),
@@ -309,6 +310,10 @@ class TreeGather:
     def rebuild_from(self, sbuf: "UVTSampleBuffer"):
         """Upload a host buffer of the same size and rebuild the hierarchy."""
         _check(load_library().tlfr_rebuild(self._h, sbuf.handle), self._h)
+
+    def trim(self):
+        """Free the hierarchy build's working storage (the hierarchy stays)."""
+        _check(load_library().tlfr_trim(self._h), self._h)
 
     def set_output(self, params: CameraParams):
         p = params._to_c(1.0, 1.0)
