@@ -103,3 +103,18 @@ def test_batch_rejects_bad_arguments():
     _torch()
     with pytest.raises(tlfr.TlfrError):
         tlfr.Batch([], [])
+
+
+def test_trim_keeps_the_hierarchy():
+    """tlfr_trim frees the build's working storage: reconstructions after it, and
+    after a rebuild that allocates it again, give the same image."""
+    _torch()
+    rec, coc = tlfr.synth_scene(tlfr.SCENE_CARDS_LARGE, 64, 40, 8, 67)
+    buf = tlfr.UVTSampleBuffer(records=rec, coc=coc)
+    g = tlfr.TreeGather(buf)
+    want = g.reconstructDofMotion()
+    g.trim()
+    assert np.array_equal(g.reconstructDofMotion().view(np.uint32), want.view(np.uint32))
+    g.rebuild_from(buf)
+    assert np.array_equal(g.reconstructDofMotion().view(np.uint32), want.view(np.uint32))
+    g.close()
