@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-rows", type=int, default=8, help="rows per CPU sample (spread over the frame)")
+    ap.add_argument("--cpu-rows", type=int, default=32, help="rows per CPU sample (spread over the frame)")
     ap.add_argument("--width", type=int, default=W)
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
@@ -185,7 +185,8 @@ class CpuSampler:
     """The reference's own CPU reconstruction (oracle/_ref; the C restatement
     when the reference build is absent) of one frame on this host's cores: the
     full hierarchy build once, then per sample a comb of rows spread over the
-    frame.  The frame time is estimated as build + (query time of the rows) x
+    frame, reconstructed in one call (the reference runs one task per scanline,
+    so the rows run in parallel on its threads).  The frame time is estimated as build + (query time of the rows) x
     height / rows.  Both the reference arm and the GPU arm's cpu_baseline use it."""
 
     def __init__(self, rec, coc, threads):
@@ -199,10 +200,9 @@ class CpuSampler:
 
     def sample(self, rows, step):
         ys = cpu_rows(self.H, rows, step)
-        t, imgs = 0.0, {}
-        for y in ys:
-            imgs[y] = self.r.reconstruct_rows(y, y + 1)[0]
-            t += self.r.last_seconds
+        img = self.r.reconstruct_rowlist(ys)
+        t = self.r.last_seconds
+        imgs = {y: img[k] for k, y in enumerate(ys)}
         est = self.build_s + t * self.H / len(ys)
         return est, t, ys, imgs
 

@@ -242,6 +242,47 @@ int ref_reconstruct_rows(void* handle, int y0, int y1, float* rgba_rows, double*
     }
 }
 
+// Reconstruct the listed scanlines rows[0..n) with the reference's per-scanline
+// task, all of them pushed to the launcher at once (so they run in parallel on
+// its threads); rgba_rows receives n*W*4 floats in list order.  Used for a CPU
+// sample of a frame's rows spread over its whole height.
+int ref_reconstruct_rowlist(void* handle, const int* rows, int n, float* rgba_rows, double* seconds)
+{
+    RefHandle* h = (RefHandle*)handle;
+    try
+    {
+        const int W = h->sbuf->getWidth();
+        TreeGather* tg = h->tg;
+        tg->generateOutputSamples(*h->params);
+        MulticoreLauncher launcher;
+        Array<TreeGather::FilterTask> ftasks;
+        ftasks.reset(n);
+        tg->m_multicore = true;
+        auto t0 = std::chrono::steady_clock::now();
+        for (int k = 0; k < n; k++)
+        {
+            ftasks[k].init(tg);
+            launcher.push(TreeGather::FilterTask::dispatcher, &ftasks[k], rows[k], 1);
+        }
+        launcher.popAll();
+        if (seconds)
+            *seconds = seconds_since(t0);
+        for (int k = 0; k < n; k++)
+            for (int x = 0; x < W; x++)
+            {
+                Vec4f c = ftasks[k].m_outputColors[x];
+                float* o = rgba_rows + ((size_t)k * W + x) * 4;
+                o[0] = c.x; o[1] = c.y; o[2] = c.z; o[3] = c.w;
+            }
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_error = e.what();
+        return 1;
+    }
+}
+
 int ref_tree_info(void* handle, int* num_nodes, int* num_samples, int* root, int* spp_pow2,
                   float* coc_adjusted, int* output_spp)
 {

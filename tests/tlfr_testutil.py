@@ -144,6 +144,23 @@ class CpuRecon:
         self.last_seconds = sec.value
         return img
 
+    def reconstruct_rowlist(self, rows):
+        """The listed rows, in one call (the reference build runs them in parallel)."""
+        rows = [int(y) for y in rows]
+        img = np.zeros((len(rows), self.W, 4), np.float32)
+        if self.kind == "ref":
+            r = np.asarray(rows, np.int32)
+            sec = ctypes.c_double()
+            assert self.lib.ref_reconstruct_rowlist(self.h, i32p(r), len(rows), f32p(img), ctypes.byref(sec)) == 0
+            self.last_seconds = sec.value
+        else:
+            t = 0.0
+            for k, y in enumerate(rows):
+                img[k] = self.reconstruct_rows(y, y + 1)[0]
+                t += self.last_seconds
+            self.last_seconds = t
+        return img
+
     def query(self, x, y, i, cap=1 << 16):
         rgba = np.zeros(4, np.float32)
         tr = np.zeros(cap, np.int32)
