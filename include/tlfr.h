@@ -67,6 +67,14 @@ typedef struct tlfr_params
     int   output_spp;        /* output samples per pixel; 0 = reference default (128, or 1 with
                                 override_uvt; Reconstruction.hpp:67-68).  Any value in [1,1024]. */
     int   device;            /* CUDA device ordinal                                              */
+    int   enable_cuda;       /* CameraParams::enableCuda, the reference's CPU/GPU toggle
+                                (CameraParams.hpp:88, Reconstruction.cpp:233): 0 (default) = the
+                                algorithm of its CPU reconstruction (TreeGather::Filterer,
+                                ReconstructionOur.cpp:50-511); 1 = the algorithm of its GPU
+                                reconstruction (first surface, wedge-box coverage, 2R surfaces
+                                with fan triangles, nearest sample; ReconstructionCuda.cpp:
+                                261-872, ReconstructionCudaKernels.cu:242-868), here with no
+                                capacity limit and no CPU overflow.  Both run on the GPU.       */
 } tlfr_params;
 
 /* Fills p with the reference defaults (CameraParams ctor, CameraParams.hpp:77-90). */

@@ -88,8 +88,14 @@ for f in "${RECON[@]}"; do
   compile "$o" "$OUT/gen_m64/reconstruction/$f" & pids+=($!)
 done
 # the driver sees private members (instrumentation only, see ref_driver.cpp)
-compile "$OUT/obj/m128/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$SRC/reconstruction_lib/reconstruction" & pids+=($!)
-compile "$OUT/obj/m64/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$OUT/gen_m64/reconstruction" & pids+=($!)
+compile "$OUT/obj/m128/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$SRC/reconstruction_lib/reconstruction" \
+  -I"$HERE/ref_shim" & pids+=($!)
+compile "$OUT/obj/m64/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$OUT/gen_m64/reconstruction" \
+  -I"$HERE/ref_shim" & pids+=($!)
+# the reference's CPU restatement of its GPU-toggle algorithm (ReconstructionCuda.cpp),
+# compiled where it lies (checker of the library's enable_cuda mode; 128 output samples)
+compile "$OUT/obj/m128/ref_gpu_toggle.o" "$HERE/ref_shim/ref_gpu_toggle.cpp" -I"$SRC/reconstruction_lib/reconstruction" \
+  -I"$HERE/ref_shim" & pids+=($!)
 # the seeded scene generator (the package's own host code, renamed), so that the
 # reference's CPU runs need no other library of this repository
 $CXX -std=c++17 -O2 -fPIC -ffp-contract=off -fno-fast-math -pthread -Dtlfr_synth_scene=ref_synth_scene -DTLFR_SYNTH_HOST_ONLY \
@@ -98,6 +104,7 @@ $CXX -std=c++17 -O2 -fPIC -ffp-contract=off -fno-fast-math -pthread -Dtlfr_synth
 for p in "${pids[@]}"; do wait "$p"; done
 objs+=("$OUT/obj/ref_synth_scene.o")
 
-$CXX -shared -pthread -o "$OUT/libtlfr_ref.so"     "${objs[@]}" "${m128[@]}" "$OUT/obj/m128/ref_driver.o"
+$CXX -shared -pthread -o "$OUT/libtlfr_ref.so"     "${objs[@]}" "${m128[@]}" "$OUT/obj/m128/ref_driver.o" \
+  "$OUT/obj/m128/ref_gpu_toggle.o"
 $CXX -shared -pthread -o "$OUT/libtlfr_ref_m64.so" "${objs[@]}" "${m64[@]}"  "$OUT/obj/m64/ref_driver.o"
 echo "built $OUT/libtlfr_ref.so $OUT/libtlfr_ref_m64.so"

@@ -21,6 +21,7 @@
 #define private public
 #define protected public
 #include "Reconstruction.hpp"
+#include "ref_handle.h"
 #undef private
 #undef protected
 
@@ -30,12 +31,6 @@ namespace
 {
 std::string g_error;
 
-struct RefHandle
-{
-    UVTSampleBuffer*    sbuf = nullptr;
-    CameraParams*       params = nullptr;
-    TreeGather*         tg = nullptr;
-};
 
 double seconds_since(std::chrono::steady_clock::time_point t0)
 {
@@ -92,14 +87,6 @@ int finish_create(RefHandle* h, float aperture, float focus, const float* uvt, i
     return 0;
 }
 } // namespace
-
-// The GPU toggle (ReconstructionCuda.cpp:876-957) needs the Fermi-era CUDA
-// runtime compiler and is not built; CameraParams::enableCuda is always false here.
-void TreeGather::cudaReconstruction(Image& resultImage, const CameraParams& params)
-{
-    (void)resultImage; (void)params;
-    fail("TreeGather::cudaReconstruction is not part of the CPU reference build");
-}
 
 extern "C" {
 

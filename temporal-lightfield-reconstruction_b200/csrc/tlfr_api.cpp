@@ -355,7 +355,7 @@ void free_ctx_buffers(tlfr::Ctx& c)
                      c.cell_count, c.cell_start, c.cell_items, c.kd, c.kd_level, c.kd_leaves_ordered, c.perm, c.box,
                      c.sbounds, c.surface, c.pending, c.leaf_task_rank, c.ordered_n, c.ordered_prefmax, c.top,
                      c.nodes, c.node_tspan, c.s_rec, c.s_col, c.s_id, c.d_pattern, c.qcol, c.heavy_queue, c.ovf_queue,
-                     c.ovf_scratch, c.coop_scratch, c.d_stats, c.d_out, c.route_fa, c.route_feats, c.route_prob,
+                     c.ovf_scratch, c.coop_scratch, c.toggle_arena, c.d_stats, c.d_out, c.route_fa, c.route_feats, c.route_prob,
                      c.route_fast, c.route_img };
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -973,6 +973,8 @@ tlfr_status tlfr_query_samples_noalloc(tlfr_ctx* ctx, const int* d_xyi, int n, f
 {
     if (!ctx || (n > 0 && (!d_xyi || !d_rgba)))
         return fail(ctx, TLFR_BAD_ARG, "tlfr_query_samples_noalloc: bad argument");
+    if (ctx->c.params.enable_cuda)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_query_samples_noalloc: the Filterer only (enable_cuda = 0)");
     tlfr::Ctx& c = ctx->c;
     cudaError_t e = cudaSetDevice(c.device);
     if (e != cudaSuccess)
@@ -984,6 +986,8 @@ tlfr_status tlfr_trace_queries(tlfr_ctx* ctx, const int* xyi, int n, float* rgba
 {
     if (!ctx || (n > 0 && (!xyi || !rgba || !trace || stride < 2)))
         return fail(ctx, TLFR_BAD_ARG, "tlfr_trace_queries: bad argument");
+    if (ctx->c.params.enable_cuda)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_trace_queries: traces follow the Filterer (enable_cuda = 0)");
     tlfr::Ctx& c = ctx->c;
     cudaSetDevice(c.device);
     for (int k = 0; k < n; k++)
@@ -1216,6 +1220,11 @@ tlfr_status tlfr_batch_create_frames(const tlfr_batch_frame* frames, int n, void
     for (int i = 0; i < n; i++)
         if (!frames[i].ctx || !frames[i].d_rgba)
             return batch_fail(nullptr, TLFR_BAD_ARG, "tlfr_batch_create: null context or output " + std::to_string(i));
+    for (int i = 0; i < n; i++)
+        if (frames[i].ctx->c.params.enable_cuda)
+            return batch_fail(nullptr, TLFR_BAD_ARG, "tlfr_batch_create: frame " + std::to_string(i) +
+                                                         " uses the GPU-toggle algorithm (enable_cuda), which batches "
+                                                         "do not run");
     const int dev = frames[0].ctx->c.device;
     for (int i = 1; i < n; i++)
         if (frames[i].ctx->c.device != dev)

@@ -170,6 +170,7 @@ struct Ctx
     float*  ovf_scratch = nullptr;  // large-capacity per-query storage
     size_t  ovf_scratch_bytes = 0;
     void*   coop_scratch = nullptr; // per-warp working lists of the cooperative full-path pass
+    void*   toggle_arena = nullptr; // large lists of the GPU-toggle algorithm's second pass
     size_t  coop_scratch_bytes = 0;
     DevStats* d_stats = nullptr;
     float4* d_out = nullptr;        // device output when the caller passes host memory

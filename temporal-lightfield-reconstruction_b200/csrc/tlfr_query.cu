@@ -1767,6 +1767,384 @@ k_query_overflow(QParams P, const int* __restrict__ queue, const int* __restrict
         flush_stats(st, ds);
 }
 
+// ---------------------------------------------------------------------------
+// The reference's GPU-toggle algorithm (CameraParams::enableCuda): its CUDA
+// kernels recKernel / failKernel / nearestKernel (ReconstructionCudaKernels.cu:
+// 242-868) and their CPU restatement CudaReconstruction::reconstructCPUSingle /
+// reconstructCPUFailed / reconstructCPUNearest (ReconstructionCuda.cpp:261-872),
+// whose semantics are followed here operation for operation, with IEEE
+// arithmetic (the reference compiles its kernels with -use_fast_math) and no
+// capacity limits: output samples that outgrow the per-thread lists run again
+// with large lists from a global arena instead of going back to the CPU.
+//   first surface at 1R: leaves with a sample within R, in order of depth at
+//     the output time; stop at the first leaf that fails sameSurface against an
+//     earlier one; coverage by the "wedge box" of the accepted samples' dx/dy
+//     slopes above and below the output sample; tent-filtered colour
+//   2R surfaces: surfaces of at least 4 samples split at sameSurface failures,
+//     each tested by the wedge boxes and a triangle fan test over every sample
+//     collected so far (the reference never clears that list)
+//   nearest: the nearest sample within R, 2R, ..., 16R (last one on ties)
+// The hierarchy's node pairs are the reference's (child0 < child1 there, so its
+// traversal, which pushes the larger index first, visits child0 first).
+// ---------------------------------------------------------------------------
+struct TStore
+{
+    int*    stack;  int stack_cap;
+    int*    leaves; int leaf_cap;
+    float2* xy;     int xy_cap;
+};
+
+// collectNodes (ReconstructionCuda.cpp:545-590): DFS, child0's subtree first;
+// leaves ordered by depth at the output time with the reference's selection
+// sort (first minimum).  Returns the leaf count or -1 when a list is full.
+TLFR_HD int toggle_collect(const QParams& P, TStore& S, const Query& o, float radius)
+{
+    int n = 0, sp = 0;
+    S.stack[sp++] = P.root;
+    while (sp > 0)
+    {
+        const int idx = S.stack[--sp];
+        const QNode node = load_node(P.nodes, idx);
+        if (!node_intersect(node, o, radius))
+            continue;
+        if (node.d.x < 0)
+        {
+            if (n == S.leaf_cap)
+                return -1;
+            S.leaves[n++] = idx;
+        }
+        else
+        {
+            if (sp + 2 > S.stack_cap)
+                return -1;
+            S.stack[sp++] = node.d.x + 1;      // child1 (the reference's idx1 after its swap: pushed first)
+            S.stack[sp++] = node.d.x;          // child0
+        }
+    }
+    for (int i = 0; i < n - 1; i++)
+    {
+        const int s0 = P.nodes[S.leaves[i]].d.z;
+        const float4 p0 = P.s_rec[2 * s0];
+        float w = p0.z + (o.t - p0.w) * P.s_rec[2 * s0 + 1].z;
+        int mn = i;
+        for (int j = i + 1; j < n; j++)
+        {
+            const int s1 = P.nodes[S.leaves[j]].d.z;
+            const float4 p1 = P.s_rec[2 * s1];
+            const float w1 = p1.z + (o.t - p1.w) * P.s_rec[2 * s1 + 1].z;
+            if (w1 < w)
+            {
+                w = w1;
+                mn = j;
+            }
+        }
+        if (mn != i)
+        {
+            const int t = S.leaves[i];
+            S.leaves[i] = S.leaves[mn];
+            S.leaves[mn] = t;
+        }
+    }
+    return n;
+}
+
+// Reprojection of sample j to the output sample (ReconstructionCuda.cpp:594-604):
+// division forms, no zero-motion shortcut.
+TLFR_HD float toggle_reproject(const QParams& P, int j, const Query& o, float& dx, float& dy)
+{
+    const float4 p = P.s_rec[2 * j];
+    const float4 m = P.s_rec[2 * j + 1];
+    const float p0x = p.x * p.z;
+    const float p0y = p.y * p.z;
+    const float p0w = p.z;
+    const float px = p0x + (o.t - p.w) * m.x;
+    const float py = p0y + (o.t - p.w) * m.y;
+    const float pw = p0w + (o.t - p.w) * m.z;
+    const float cocr = P.c0 / pw + P.c1;
+    const float x = px / pw + cocr * o.u;
+    const float y = py / pw + cocr * o.v;
+    dx = x - o.x;
+    dy = y - o.y;
+    return dx * dx + dy * dy;
+}
+
+// sameSurface of the GPU toggle (ReconstructionCuda.cpp:127-190): the same
+// sixteen plane comparisons as the Filterer's.
+TLFR_HD bool toggle_same(const QParams& P, int a, int b, const Query& o)
+{
+    const float RANGE = 1.0f / sqrtf(128.0f);
+    const float uvtmin[3] = { o.u - RANGE, o.v - RANGE, o.t - 0.5f * RANGE };
+    const float uvtmax[3] = { o.u + RANGE, o.v + RANGE, o.t + 0.5f * RANGE };
+    return same_surface(load_node(P.nodes, a), load_node(P.nodes, b), uvtmin, uvtmax);
+}
+
+TLFR_HD void wbox_add(float* box, float dx, float dy)
+{
+    const float k = dx / dy;
+    if (dy >= 0.f)
+    {
+        box[0] = minr(box[0], k);
+        box[1] = maxr(box[1], k);
+    }
+    else
+    {
+        box[2] = minr(box[2], k);
+        box[3] = maxr(box[3], k);
+    }
+}
+
+// checkTriangles (ReconstructionCuda.cpp:193-219) over offsets from the output sample.
+TLFR_HD bool toggle_triangles(const float2* xy, int n, float dispersion)
+{
+    for (int m = 0; m < n - 2; m++)
+        for (int k = m + 1; k < n - 1; k++)
+            for (int l = k + 1; l < n; l++)
+            {
+                const float2 p0 = xy[m], p1 = xy[k], p2 = xy[l];
+                if (len2(p0.x - p1.x, p0.y - p1.y) > 2 * dispersion || len2(p1.x - p2.x, p1.y - p2.y) > 2 * dispersion ||
+                    len2(p2.x - p0.x, p2.y - p0.y) > 2 * dispersion)
+                    continue;
+                const float c0 = p0.x * p1.y - p1.x * p0.y;
+                const float c1 = p1.x * p2.y - p2.x * p1.y;
+                const float c2 = p2.x * p0.y - p0.x * p2.y;
+                if (c0 <= 0.f && c1 <= 0.f && c2 <= 0.f)
+                    return true;
+                if (c0 >= 0.f && c1 >= 0.f && c2 >= 0.f)
+                    return true;
+            }
+    return false;
+}
+
+// reconstructCPUNearest (ReconstructionCuda.cpp:700-744).  false when a list is full.
+TLFR_HD bool toggle_nearest(const QParams& P, TStore& S, const Query& o, float4& out)
+{
+    for (float rmul = 1.f; rmul <= 16.f; rmul *= 2.f)
+    {
+        const float radius = rmul * P.disp0;
+        const int n = toggle_collect(P, S, o, radius);
+        if (n < 0)
+            return false;
+        int minIdx = -1;
+        float minDist = kF32Max;
+        for (int i = 0; i < n; i++)
+        {
+            const int4 d = P.nodes[S.leaves[i]].d;
+            for (int j = d.z; j < d.w; j++)
+            {
+                float dx, dy;
+                const float dist2 = toggle_reproject(P, j, o, dx, dy);
+                if (dist2 <= minDist)
+                {
+                    minDist = dist2;
+                    minIdx = j;
+                }
+            }
+        }
+        if (minIdx >= 0)
+        {
+            out = P.s_col[minIdx];
+            return true;
+        }
+    }
+    out = make_float4(0, 0, 0, 0);
+    return true;
+}
+
+// reconstructCPUFailed (ReconstructionCuda.cpp:748-872).  false when a list is full.
+TLFR_HD bool toggle_failed(const QParams& P, TStore& S, const Query& o, float4& out)
+{
+    const float dispersion = P.disp0;
+    const float radius = 2.f * dispersion;
+    const int nleaves = toggle_collect(P, S, o, radius);
+    if (nleaves < 0)
+        return false;
+    if (nleaves == 0)
+        return toggle_nearest(P, S, o, out);
+    int nxy = 0, numPoints = 0, sfirst = 0, lidx = 0;
+    float4 color = make_float4(0, 0, 0, 0);
+    const int MIN_SAMPLES_PER_SURFACE = 4;
+    do
+    {
+        sfirst = lidx;
+        numPoints = 0;
+        color = make_float4(0, 0, 0, 0);
+        float abox[4] = { kF32Max, -kF32Max, kF32Max, -kF32Max };
+        float wbox[4] = { kF32Max, -kF32Max, kF32Max, -kF32Max };
+        do
+        {
+            const int leaf = S.leaves[lidx];
+            bool endSurface = false;
+            if (numPoints >= MIN_SAMPLES_PER_SURFACE)
+                for (int j = sfirst; j < lidx; ++j)
+                    if (!toggle_same(P, leaf, S.leaves[j], o))
+                    {
+                        endSurface = true;
+                        break;
+                    }
+            if (endSurface)
+                break;
+            const int4 d = P.nodes[leaf].d;
+            for (int i = d.z; i < d.w; i++)
+            {
+                float dx, dy;
+                const float dist2 = toggle_reproject(P, i, o, dx, dy);
+                if (dist2 <= radius * radius)
+                {
+                    if (nxy == S.xy_cap)
+                        return false;
+                    S.xy[nxy++] = make_float2(dx, dy);
+                    numPoints++;
+                    const float w = 1.f - sqrtf(dist2) / dispersion;
+                    if (w <= 0.f)
+                        wbox_add(abox, dx, dy);
+                    else
+                    {
+                        wbox_add(wbox, dx, dy);
+                        const float4 c = P.s_col[i];
+                        color.x += w * c.x; color.y += w * c.y; color.z += w * c.z; color.w += w * c.w;
+                    }
+                }
+            }
+            lidx++;
+        } while (lidx < nleaves);
+        if (lidx < nleaves)
+        {
+            abox[0] = minr(abox[0], wbox[0]);
+            abox[1] = maxr(abox[1], wbox[1]);
+            abox[2] = minr(abox[2], wbox[2]);
+            abox[3] = maxr(abox[3], wbox[3]);
+            if (abox[1] > abox[2] && abox[0] < abox[3])
+                if ((wbox[1] > wbox[2] && wbox[0] < wbox[3]) || toggle_triangles(S.xy, nxy, dispersion))
+                    break;
+        }
+    } while (lidx < nleaves);
+    if (color.w > 0.f)
+    {
+        const float r = 1.f / color.w;
+        out = make_float4(color.x * r, color.y * r, color.z * r, color.w * r);
+        return true;
+    }
+    return toggle_nearest(P, S, o, out);
+}
+
+// reconstructCPUSingle (ReconstructionCuda.cpp:592-698).  false when a list is full.
+TLFR_HD bool toggle_single(const QParams& P, TStore& S, const Query& o, float4& out)
+{
+    const float radius = P.disp0;
+    int n = toggle_collect(P, S, o, radius);
+    if (n < 0)
+        return false;
+    // leaves without a sample within R are dropped
+    int lcount = 0;
+    for (int i = 0; i < n; i++)
+    {
+        const int4 d = P.nodes[S.leaves[i]].d;
+        bool empty = true;
+        for (int j = d.z; j < d.w && empty; j++)
+        {
+            float dx, dy;
+            if (toggle_reproject(P, j, o, dx, dy) <= radius * radius)
+                empty = false;
+        }
+        if (!empty)
+            S.leaves[lcount++] = S.leaves[i];
+    }
+    n = lcount;
+    if (n == 0)
+        return toggle_failed(P, S, o, out);
+    float wbox[4] = { kF32Max, -kF32Max, kF32Max, -kF32Max };
+    bool multi = false;
+    float4 color = make_float4(0, 0, 0, 0);
+    for (int i = 0; i < n; i++)
+    {
+        for (int j = 0; j < i; j++)
+            if (!toggle_same(P, S.leaves[i], S.leaves[j], o))
+            {
+                multi = true;
+                break;
+            }
+        if (multi)
+            break;
+        const int4 d = P.nodes[S.leaves[i]].d;
+        for (int j = d.z; j < d.w; j++)
+        {
+            float dx, dy;
+            const float dist2 = toggle_reproject(P, j, o, dx, dy);
+            if (dist2 <= radius * radius)
+            {
+                wbox_add(wbox, dx, dy);
+                const float w = maxr(0.f, 1.f - sqrtf(dist2) / radius);
+                const float4 c = P.s_col[j];
+                color.x += w * c.x; color.y += w * c.y; color.z += w * c.z; color.w += w * c.w;
+            }
+        }
+    }
+    if (color.w > 0.f && wbox[1] > wbox[2] && wbox[0] < wbox[3])
+    {
+        const float r = 1.f / color.w;
+        out = make_float4(color.x * r, color.y * r, color.z * r, color.w * r);
+        return true;
+    }
+    if (multi)
+        return toggle_failed(P, S, o, out);
+    return toggle_nearest(P, S, o, out);
+}
+
+constexpr int kTgStack = 128, kTgLeaf = 256, kTgXy = 512;
+
+// Every output sample of the frame, one thread each, lists in local memory;
+// output samples that outgrow them are queued for k_toggle_large.
+__global__ void __launch_bounds__(kBlock)
+k_toggle(QParams P, long long num_queries, float4* __restrict__ qcol, int* __restrict__ ovf_queue,
+         int* __restrict__ ovf_count, int ovf_cap)
+{
+    int stack[kTgStack];
+    int leaves[kTgLeaf];
+    float2 xy[kTgXy];
+    TStore S{ stack, kTgStack, leaves, kTgLeaf, xy, kTgXy };
+    for (long long q = blockIdx.x * (long long)kBlock + threadIdx.x; q < num_queries; q += (long long)gridDim.x * kBlock)
+    {
+        float4 c;
+        if (toggle_single(P, S, query_of(P, q), c))
+            qcol[q] = c;
+        else
+        {
+            const int slot = atomicAdd(ovf_count, 1);
+            if (slot < ovf_cap)
+                ovf_queue[slot] = (int)q;
+        }
+    }
+}
+
+// The queued output samples with large lists from a global arena (one slot
+// per thread); a sample that outgrows those too is counted as a hard failure.
+__global__ void __launch_bounds__(64)
+k_toggle_large(QParams P, const int* __restrict__ queue, const int* __restrict__ count_ptr, int cap,
+               float4* __restrict__ qcol, char* arena, size_t slot_bytes, int num_slots, int stack_cap, int leaf_cap,
+               int xy_cap, int* hard_fail)
+{
+    const int count = min(*count_ptr, cap);
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= num_slots)
+        return;
+    char* base = arena + (size_t)slot * slot_bytes;
+    TStore S;
+    S.stack = (int*)base;                       S.stack_cap = stack_cap;
+    S.leaves = S.stack + stack_cap;             S.leaf_cap = leaf_cap;
+    S.xy = (float2*)(S.leaves + leaf_cap);      S.xy_cap = xy_cap;
+    for (int k = slot; k < count; k += num_slots)
+    {
+        const int q = queue[k];
+        float4 c;
+        if (!toggle_single(P, S, query_of(P, q), c))
+        {
+            atomicAdd(hard_fail, 1);
+            c = make_float4(0, 0, 0, 0);
+        }
+        qcol[q] = c;
+    }
+}
+
 // Pixel = sum of its output samples in sample order, times rcp(alpha); red
 // when empty (Reconstruction.cpp:665-719).
 __global__ void k_resolve(const float4* __restrict__ qcol, int M, float4* __restrict__ out, long long npix)
@@ -2382,6 +2760,71 @@ tlfr_status batch_failures(BatchPlan& bp, cudaStream_t s, std::vector<int>& hard
     return TLFR_OK;
 }
 
+// capacities of the GPU-toggle algorithm's large pass (one arena slot per thread)
+constexpr int kTgLargeStack = 512, kTgLargeLeaf = 8192, kTgLargeXy = 32768, kTgLargeSlots = 512;
+
+static size_t toggle_slot_bytes()
+{
+    const size_t b = sizeof(int) * (kTgLargeStack + kTgLargeLeaf) + sizeof(float2) * kTgLargeXy;
+    return (b + 255) & ~(size_t)255;
+}
+
+// A frame with the reference's GPU-toggle algorithm (enable_cuda): every output
+// sample with per-thread lists, the ones that outgrew them with large lists,
+// then the pixel resolve.
+static tlfr_status reconstruct_toggle(Ctx& c, float4* d_rgba)
+{
+    cudaStream_t s = c.stream;
+    const long long npix = (long long)c.W * c.H;
+    const long long nq = npix * c.out_spp;
+    int* counters = reinterpret_cast<int*>(c.d_stats + 1);
+    QParams P = make_params(c);
+    CKQ(cudaMemsetAsync(c.d_stats, 0, sizeof(DevStats) + 8 * sizeof(int), s));
+    if (!c.evq0)
+    {
+        CKQ(cudaEventCreate(&c.evq0));
+        CKQ(cudaEventCreate(&c.evq1));
+        CKQ(cudaEventCreate(&c.evq2));
+    }
+    CKQ(cudaEventRecord(c.evq0, s));
+    const int blocks = (int)std::min<long long>((nq + kBlock - 1) / kBlock, (long long)c.num_sms * 16);
+    TLFR_LAUNCH(c, k_toggle, blocks, kBlock, s, P, nq, c.qcol, c.ovf_queue, counters + 0, (int)c.ovf_cap);
+    CKQ(cudaEventRecord(c.evq1, s));
+    int novf = 0;
+    CKQ(cudaMemcpyAsync(&novf, counters + 0, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CKQ(cudaStreamSynchronize(s));
+    int hard = 0;
+    if (novf > 0)
+    {
+        if (!c.toggle_arena)
+            CKQ(cudaMalloc(&c.toggle_arena, toggle_slot_bytes() * kTgLargeSlots));
+        const int slots = std::min(kTgLargeSlots, novf);
+        TLFR_LAUNCH(c, k_toggle_large, (slots + 63) / 64, 64, s, P, c.ovf_queue, counters + 0, (int)c.ovf_cap, c.qcol,
+                    (char*)c.toggle_arena, toggle_slot_bytes(), slots, kTgLargeStack, kTgLargeLeaf, kTgLargeXy,
+                    counters + 1);
+        CKQ(cudaMemcpyAsync(&hard, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    }
+    CKQ(cudaEventRecord(c.evq2, s));
+    TLFR_LAUNCH(c, k_resolve, (int)std::min<long long>((npix + 127) / 128, (long long)c.num_sms * 32), 128, s, c.qcol,
+                c.out_spp, d_rgba, npix);
+    CKQ(cudaGetLastError());
+    CKQ(cudaStreamSynchronize(s));
+    float ms = 0, ms2 = 0;
+    CKQ(cudaEventElapsedTime(&ms, c.evq0, c.evq1));
+    CKQ(cudaEventElapsedTime(&ms2, c.evq1, c.evq2));
+    c.last.light_ms = ms;
+    c.last.heavy_ms = ms2;
+    c.last.query_kernel_ms = ms + ms2;
+    c.last.num_overflow_queries = novf;
+    c.last.num_heavy_queries = novf;
+    if (hard > 0)
+    {
+        c.error = "a query exceeded the largest supported capacity";
+        return TLFR_OVERFLOW;
+    }
+    return TLFR_OK;
+}
+
 tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
 {
     cudaStream_t s = c.stream;
@@ -2406,6 +2849,8 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
     }
     if (!c.d_stats)
         CKQ(cudaMalloc(&c.d_stats, sizeof(DevStats) + 8 * sizeof(int)));
+    if (c.params.enable_cuda)
+        return reconstruct_toggle(c, d_rgba);
     int* counters = reinterpret_cast<int*>(c.d_stats + 1);   // [0] overflow, [1] hard, [2] heavy
     QParams P = make_params(c);
     CKQ(cudaMemsetAsync(c.d_stats, 0, sizeof(DevStats) + 8 * sizeof(int), s));

@@ -51,6 +51,7 @@ class _Params(ctypes.Structure):
         ("uvt", ctypes.c_float * 3),
         ("output_spp", ctypes.c_int),
         ("device", ctypes.c_int),
+        ("enable_cuda", ctypes.c_int),
     ]
 
 
@@ -236,20 +237,21 @@ class UVTSampleBuffer:
 class CameraParams:
     """The CameraParams fields the reconstruction path reads (CameraParams.hpp:74-107).
 
-    enableCuda selects the reference's CPU/GPU toggle; this library only has the
-    GPU side, so it must stay True.  overrideUVT: None or (u, v, t); the t=1
-    pinhole image is (0, 0, 1) (reconstruction_app/App.cpp:450).
+    enableCuda is the reference's CPU/GPU toggle (CameraParams.hpp:88): False (its
+    default) selects the algorithm of the reference's CPU reconstruction
+    (TreeGather::Filterer), True the algorithm of its GPU reconstruction
+    (ReconstructionCuda.cpp / ReconstructionCudaKernels.cu).  This library runs
+    both on the GPU.  overrideUVT: None or (u, v, t); the t=1 pinhole image is
+    (0, 0, 1) (reconstruction_app/App.cpp:450).
     """
     lensFilter: int = LENS_BOX
     timeFilter: int = TIME_BOX
     overrideUVT: Optional[Tuple[float, float, float]] = None
-    enableCuda: bool = True
+    enableCuda: bool = False
     outputSpp: int = 0          # 0: reference default (128, or 1 with overrideUVT)
     device: int = 0
 
     def _to_c(self, aperture: float, focus: float) -> _Params:
-        if not self.enableCuda:
-            raise ValueError("enableCuda=False selects the CPU reconstruction, which this library does not provide")
         p = _Params()
         load_library().tlfr_params_default(ctypes.byref(p))
         p.aperture_adjust = aperture
@@ -261,6 +263,7 @@ class CameraParams:
             p.uvt[0], p.uvt[1], p.uvt[2] = self.overrideUVT
         p.output_spp = self.outputSpp
         p.device = self.device
+        p.enable_cuda = 1 if self.enableCuda else 0
         return p
 
 

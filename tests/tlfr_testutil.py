@@ -161,6 +161,24 @@ class CpuRecon:
             self.last_seconds = t
         return img
 
+    def gpu_toggle_image(self):
+        """The reference's CPU restatement of its GPU-toggle algorithm over the whole
+        image (CudaReconstruction::reconstructCPU, reference build only)."""
+        assert self.kind == "ref"
+        img = np.zeros((self.H, self.W, 4), np.float32)
+        sec = ctypes.c_double()
+        assert self.lib.ref_gpu_toggle_image(self.h, f32p(img), ctypes.byref(sec)) == 0
+        self.last_seconds = sec.value
+        return img
+
+    def gpu_toggle_queries(self, xyi):
+        """Output samples (x, y, i) through CudaReconstruction::reconstructCPUSingle."""
+        assert self.kind == "ref"
+        q = np.ascontiguousarray(np.asarray(xyi, np.int32).reshape(-1, 3))
+        out = np.zeros((len(q), 4), np.float32)
+        assert self.lib.ref_gpu_toggle_queries(self.h, i32p(q), len(q), f32p(out)) == 0
+        return out
+
     def query(self, x, y, i, cap=1 << 16):
         rgba = np.zeros(4, np.float32)
         tr = np.zeros(cap, np.int32)
