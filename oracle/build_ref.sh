@@ -91,7 +91,7 @@ done
 compile "$OUT/obj/m128/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$SRC/reconstruction_lib/reconstruction" \
   -I"$HERE/ref_shim" & pids+=($!)
 compile "$OUT/obj/m64/ref_driver.o" "$HERE/ref_shim/ref_driver.cpp" -I"$OUT/gen_m64/reconstruction" \
-  -I"$HERE/ref_shim" & pids+=($!)
+  -I"$HERE/ref_shim" -DTLFR_REF_NO_GPU_TOGGLE & pids+=($!)
 # the reference's CPU restatement of its GPU-toggle algorithm (ReconstructionCuda.cpp),
 # compiled where it lies (checker of the library's enable_cuda mode; 128 output samples)
 compile "$OUT/obj/m128/ref_gpu_toggle.o" "$HERE/ref_shim/ref_gpu_toggle.cpp" -I"$SRC/reconstruction_lib/reconstruction" \

@@ -88,6 +88,16 @@ int finish_create(RefHandle* h, float aperture, float focus, const float* uvt, i
 }
 } // namespace
 
+#ifdef TLFR_REF_NO_GPU_TOGGLE
+// The 64-output-sample variant does not carry the GPU-toggle translation unit
+// (ref_gpu_toggle.cpp); CameraParams::enableCuda is always false there.
+void TreeGather::cudaReconstruction(Image& resultImage, const CameraParams& params)
+{
+    (void)resultImage; (void)params;
+    fail("TreeGather::cudaReconstruction is not part of this build");
+}
+#endif
+
 extern "C" {
 
 const char* ref_last_error(void) { return g_error.c_str(); }
