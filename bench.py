@@ -78,6 +78,8 @@ def parse():
                     help="time the query passes of one frame (--width/--height/--spp, --steps/--warmup) and print "
                          "one JSON line; the entry point for profiler captures")
     ap.add_argument("--scene", type=int, default=PRESET, help="scene preset of --profile-frame")
+    ap.add_argument("--enable-cuda", action="store_true",
+                    help="--profile-frame with the reference's GPU-toggle algorithm (CameraParams.enableCuda)")
     return ap.parse_args()
 
 
@@ -484,7 +486,7 @@ def run_profile_frame(args):
     rec, coc = tlfr.synth_scene(args.scene, Wd, Hd, S, 2)
     d_rec = torch.from_numpy(rec).cuda()
     stream = torch.cuda.current_stream()
-    tg = tlfr.TreeGather(None, tlfr.CameraParams(device=0), stream=stream.cuda_stream,
+    tg = tlfr.TreeGather(None, tlfr.CameraParams(device=0, enableCuda=args.enable_cuda), stream=stream.cuda_stream,
                          device_records=(d_rec.data_ptr(), (Wd, Hd, S), coc))
     out = torch.empty((Hd, Wd, 4), dtype=torch.float32, device="cuda")
     rows = []
@@ -498,6 +500,7 @@ def run_profile_frame(args):
     torch.cuda.synchronize()
     med = lambda i: statistics.median(r[i] for r in rows)
     line = {"profile_frame": f"{Wd}x{Hd}x{S}", "scene": args.scene, "steps": args.steps, "warmup": args.warmup,
+            "algorithm": "gpu toggle (enableCuda)" if args.enable_cuda else "filterer",
             "build_ms": med(0), "light_ms": med(1), "heavy_ms": med(2), "query_kernel_ms": med(3),
             "heavy_queries": int(rows[-1][4]), "output_samples": Wd * Hd * M,
             "checksum": float(out.double().sum().item())}
