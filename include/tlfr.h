@@ -200,6 +200,21 @@ int tlfr_output_samples(tlfr_ctx* ctx, float* out5);
  * with tlfr_buffer_free.                                                     */
 tlfr_status tlfr_output_sample_buffer(tlfr_ctx* ctx, tlfr_buffer** out);
 
+/* Shadow reconstruction, TreeGather::reconstructShadows (Reconstruction.cpp:
+ * 302-344; the reference notes it is not callable from its application): the
+ * context's hierarchy holds light-space samples (their dw/dx, dw/dy in record
+ * fields 14-15); each of the n query samples (16-float records of the view in
+ * light space: x, y, w, u, v, t are read, fields 0,1,3,4,5,6) runs the Filterer
+ * in shadow mode (ReconstructionOur.cpp:78-80, 283-291, 337-347): dispersion
+ * scaled by sqrt(density[k]) (the query buffer's LIGHTSPACE_DENSITY channel;
+ * NULL reads 1), each filtered sample's colour kept where it lights the query
+ * (w - 0.01 <= sample w at t + (query - sample) . (dw/dx, dw/dy)) and black
+ * with its alpha where it shadows it, no lens or time weights.  rgba receives
+ * 4 floats per query (host memory); the reference writes them into the query
+ * buffer's sample colours.  Host buffers; synchronous.                       */
+tlfr_status tlfr_reconstruct_shadows(tlfr_ctx* ctx, const float* queries16, int num_queries, const float* density,
+                                     float* rgba);
+
 /* Run the output samples (x, y, i) listed in xyi[3*k ..] through the device query
  * path with tracing on.  rgba[4*k ..] = the query colour.  trace[k*trace_stride ..]:
  *   [0] flags: bit0 = 2R fetch, bit1 = widened beyond 2R, bit2 = surfaces merged,

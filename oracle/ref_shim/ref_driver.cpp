@@ -280,6 +280,43 @@ int ref_reconstruct_rowlist(void* handle, const int* rows, int n, float* rgba_ro
     }
 }
 
+// TreeGather::reconstructShadows (Reconstruction.cpp:302-344) with a query buffer of
+// the light buffer's size and qspp samples per pixel (16-float records, pixel-major)
+// and its LIGHTSPACE_DENSITY channel; rgba receives the query buffer's sample
+// colours afterwards (W*H*qspp*4).
+int ref_reconstruct_shadows(void* handle, const float* queries, int qspp, const float* density, float* rgba)
+{
+    RefHandle* h = (RefHandle*)handle;
+    try
+    {
+        const int W = h->sbuf->getWidth(), H = h->sbuf->getHeight();
+        UVTSampleBuffer* q = buffer_from_records(queries, W, H, qspp, 0.0f, 0.0f);
+        const int cid = q->reserveChannel<float>("LIGHTSPACE_DENSITY");
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++)
+                for (int i = 0; i < qspp; i++)
+                    (*(Array<float>*)(q->m_channels[cid]))[q->getIndex(x, y, i)] =
+                        density[((size_t)y * W + x) * qspp + i];
+        h->tg->reconstructShadows(q, NULL);
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++)
+                for (int i = 0; i < qspp; i++)
+                {
+                    const Vec4f c = q->getSampleColor(x, y, i);
+                    float* o = rgba + (((size_t)y * W + x) * qspp + i) * 4;
+                    o[0] = c.x; o[1] = c.y; o[2] = c.z; o[3] = c.w;
+                }
+        h->tg->m_qbuf = NULL;
+        delete q;
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_error = e.what();
+        return 1;
+    }
+}
+
 int ref_tree_info(void* handle, int* num_nodes, int* num_samples, int* root, int* spp_pow2,
                   float* coc_adjusted, int* output_spp)
 {

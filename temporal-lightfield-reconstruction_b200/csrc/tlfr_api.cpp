@@ -919,6 +919,55 @@ int tlfr_output_samples(tlfr_ctx* ctx, float* out5)
     return (int)(ctx->c.h_pattern.size() / 5);
 }
 
+// TreeGather::reconstructShadows (Reconstruction.cpp:302-344) for a flat list of
+// light-space query samples.
+tlfr_status tlfr_reconstruct_shadows(tlfr_ctx* ctx, const float* queries16, int n, const float* density, float* rgba)
+{
+    if (!ctx || n < 0 || (n > 0 && (!queries16 || !rgba)))
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_reconstruct_shadows: bad argument");
+    tlfr::Ctx& c = ctx->c;
+    if (c.params.enable_cuda)
+        return fail(ctx, TLFR_BAD_ARG, "tlfr_reconstruct_shadows: the Filterer only (enable_cuda = 0)");
+    if (n == 0)
+        return TLFR_OK;
+    cudaSetDevice(c.device);
+    std::vector<float> q8((size_t)n * 8);
+    for (int k = 0; k < n; k++)
+    {
+        const float* e = queries16 + (size_t)k * 16;
+        float* d = &q8[(size_t)k * 8];
+        d[0] = e[0]; d[1] = e[1]; d[2] = e[4]; d[3] = e[5]; d[4] = e[6]; d[5] = e[3];
+        d[6] = density ? density[k] : 1.0f;
+        d[7] = 0.0f;
+    }
+    float* d_q = nullptr;
+    float4* d_out = nullptr;
+    if (cudaMalloc(&d_q, sizeof(float) * q8.size()) != cudaSuccess ||
+        cudaMalloc(&d_out, sizeof(float4) * (size_t)n) != cudaSuccess)
+    {
+        cudaFree(d_q);
+        return fail(ctx, TLFR_OOM, "tlfr_reconstruct_shadows: allocation failed");
+    }
+    tlfr_status st = TLFR_OK;
+    if (cudaMemcpyAsync(d_q, q8.data(), sizeof(float) * q8.size(), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+        st = fail(ctx, TLFR_CUDA, "tlfr_reconstruct_shadows: upload failed");
+    if (st == TLFR_OK)
+    {
+        st = tlfr::reconstruct_shadows(c, d_q, n, d_out);
+        if (st != TLFR_OK)
+            st = fail(ctx, st, "tlfr_reconstruct_shadows: %s", c.error.c_str());
+    }
+    if (st == TLFR_OK)
+    {
+        if (cudaMemcpyAsync(rgba, d_out, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+            cudaStreamSynchronize(c.stream) != cudaSuccess)
+            st = fail(ctx, TLFR_CUDA, "tlfr_reconstruct_shadows: download failed");
+    }
+    cudaFree(d_q);
+    cudaFree(d_out);
+    return st;
+}
+
 // The reconstruction's output-sample buffer (the m_obuf debug dump,
 // Reconstruction.cpp:290-294, 696-712): one record per output sample (x, y, i)
 // with the sample's position, lens and time coordinates and its reconstructed

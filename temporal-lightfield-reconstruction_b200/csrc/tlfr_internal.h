@@ -254,6 +254,8 @@ int light_default_blocks(const Ctx& c);
 size_t overflow_scratch_bytes();
 size_t coop_scratch_bytes(int num_sms);
 tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h_trace, int stride);
+// shadow reconstruction of n light-space queries (8 floats each, device) into d_out (device)
+tlfr_status reconstruct_shadows(Ctx& c, const float* d_queries, int n, float4* d_out);
 // output samples through the full path with working storage in a fixed device array
 tlfr_status query_samples_noalloc(Ctx& c, const int* d_xyi, int n, float* d_rgba, int* d_overflow);
 // host-side output pattern (Reconstruction.cpp:452-512)

@@ -314,13 +314,39 @@ TLFR_HD float gaussian(float x, float stddev, float mean)
     return powf(e, -((x - mean) * (x - mean)) / (2.0f * (stddev * stddev)));
 }
 
+// A shadow query (TreeGather::reconstructShadows, R.cpp:302-344): the light-space
+// depth of the query and the input samples' depth gradients (dw/dx, dw/dy per
+// tree-ordered sample), against which each filtered sample's visibility is
+// tested (RO.cpp:283-291, 337-347).
+struct ShadowQ
+{
+    float w;                    // query's w
+    float dispersion;           // dispersion * sqrt(light-space density) (RO.cpp:78-80)
+    const float2* wg;           // per tree-ordered sample
+};
+
+constexpr float kShadowBias = 0.01f;     // SHADOW_BIAS (RO.cpp:46)
+
+// w of sample i at time t (the ReconSample key of collectInputSamples2)
+TLFR_HD float sample_w_at(const QParams& P, int i, float t)
+{
+    const float4 sp4 = P.s_rec[2 * i];
+    const float4 sm = P.s_rec[2 * i + 1];
+    if (sm.x != 0.0f || sm.y != 0.0f || sm.z != 0.0f)
+        return (1.0f * sp4.z) + sm.z * (t - sp4.w);
+    return sp4.z;
+}
+
 // Filterer::reconstruct (RO.cpp:50-359).  trace, when given, receives the
-// flags and the final surfaces (layout documented in tlfr.h).
+// flags and the final surfaces (layout documented in tlfr.h).  sh, when given,
+// makes it the shadow reconstruction: the dispersion scaled by the light-space
+// density, each filtered sample's colour kept where the query is lit by it and
+// (0, 0, 0, alpha) where it is shadowed, no lens or time weights.
 template <bool TRACE>
 TLFR_HD int reconstruct_query(const QParams& P, Store& S, const Query& o, QStats& st, float4& out,
-                                 int* trace, int trace_cap)
+                                 int* trace, int trace_cap, const ShadowQ* sh = nullptr)
 {
-    float dispersion = P.disp0;
+    float dispersion = sh ? sh->dispersion : P.disp0;
     int nsurf = 0;
     int flags = 0;
     int n1 = collect(P, S, o, dispersion, nsurf, st);
@@ -439,7 +465,15 @@ TLFR_HD int reconstruct_query(const QParams& P, Store& S, const Query& o, QStats
                 const float weight = 1 - len2(dx, dy) / dispersion;
                 if (weight <= 0)
                     continue;
-                const float4 c = P.s_col[r.index];
+                float4 c = P.s_col[r.index];
+                if (sh)
+                {
+                    const float2 g = sh->wg[r.index];
+                    const float key = sample_w_at(P, r.index, o.t);
+                    const bool lit = sh->w - kShadowBias <= key + (dx * g.x + dy * g.y);
+                    if (!lit)
+                        c = make_float4(0, 0, 0, c.w);
+                }
                 res.x += c.x * weight;
                 res.y += c.y * weight;
                 res.z += c.z * weight;
@@ -478,6 +512,19 @@ TLFR_HD int reconstruct_query(const QParams& P, Store& S, const Query& o, QStats
     {
         const RSample na = S.rs[S.surf[nearS].start + nearI];
         res = P.s_col[na.index];
+        if (sh)
+        {
+            const float2 g = sh->wg[na.index];
+            const float dx = o.x - na.x, dy = o.y - na.y;
+            const bool lit = sh->w - kShadowBias <= sample_w_at(P, na.index, o.t) + (dx * g.x + dy * g.y);
+            if (!lit)
+                res = make_float4(0, 0, 0, res.w);
+        }
+    }
+    if (sh)
+    {
+        out = res;
+        return kQOk;
     }
     if (P.lens_filter == 1)
     {
@@ -2145,6 +2192,97 @@ k_toggle_large(QParams P, const int* __restrict__ queue, const int* __restrict__
     }
 }
 
+// overflow pass capacities
+constexpr int kOvStack = 512, kOvLeaf = 16384, kOvRs = 65536, kOvSurf = 4096;
+constexpr int kOvSlots = 4096;
+
+// ---------------------------------------------------------------------------
+// Shadow reconstruction (TreeGather::reconstructShadows, R.cpp:302-344): the
+// hierarchy holds light-space samples; each query is a light-space sample of
+// the view (x, y, u, v, t, w and its light-space density) and receives, from
+// the Filterer in shadow mode, the colour of the samples that light it
+// (RO.cpp:78-80, 283-291, 337-347).  Queries are 8 floats: x, y, u, v, t, w,
+// density, unused.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ Query shadow_query(const float* q8, float& w, float& density)
+{
+    Query o;
+    o.x = q8[0]; o.y = q8[1]; o.u = q8[2]; o.v = q8[3]; o.t = q8[4];
+    w = q8[5];
+    density = q8[6];
+    return o;
+}
+
+// dw/dx, dw/dy of every tree-ordered sample from its input record
+__global__ void k_gather_wg(const float* __restrict__ records, const int* __restrict__ s_id, int n,
+                            float2* __restrict__ wg)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    {
+        const float* r = records + (size_t)s_id[k] * 16;
+        wg[k] = make_float2(r[14], r[15]);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_query_shadow(QParams P, const float* __restrict__ queries, int n, const float2* __restrict__ wg,
+               float4* __restrict__ out, int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap)
+{
+    int stack[kStackCap];
+    Leaf leaves[kLeafCap];
+    RSample rs[kRsCap];
+    Surf surf[kSurfCap];
+    Store S{ stack, kStackCap, leaves, kLeafCap, rs, kRsCap, surf, kSurfCap };
+    for (int k = blockIdx.x * kBlock + threadIdx.x; k < n; k += gridDim.x * kBlock)
+    {
+        float w, density;
+        const Query o = shadow_query(queries + 8 * (size_t)k, w, density);
+        const ShadowQ sh{ w, P.disp0 * sqrtf(density), wg };
+        QStats qs{};
+        float4 c;
+        if (reconstruct_query<false>(P, S, o, qs, c, nullptr, 0, &sh) == kQOk)
+            out[k] = c;
+        else
+        {
+            const int slot = atomicAdd(ovf_count, 1);
+            if (slot < ovf_cap)
+                ovf_queue[slot] = k;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(64)
+k_query_shadow_large(QParams P, const float* __restrict__ queries, const int* __restrict__ queue,
+                     const int* __restrict__ count_ptr, int cap, const float2* __restrict__ wg, float4* __restrict__ out,
+                     char* arena, size_t slot_bytes, int num_slots, int* hard_fail)
+{
+    const int count = min(*count_ptr, cap);
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= num_slots)
+        return;
+    char* base = arena + (size_t)slot * slot_bytes;
+    Store S;
+    S.stack = (int*)base;                      S.stack_cap = kOvStack;
+    S.leaves = (Leaf*)(S.stack + kOvStack);    S.leaf_cap = kOvLeaf;
+    S.rs = (RSample*)(S.leaves + kOvLeaf);     S.rs_cap = kOvRs;
+    S.surf = (Surf*)(S.rs + kOvRs);            S.surf_cap = kOvSurf;
+    for (int j = slot; j < count; j += num_slots)
+    {
+        const int k = queue[j];
+        float w, density;
+        const Query o = shadow_query(queries + 8 * (size_t)k, w, density);
+        const ShadowQ sh{ w, P.disp0 * sqrtf(density), wg };
+        QStats qs{};
+        float4 c;
+        if (reconstruct_query<false>(P, S, o, qs, c, nullptr, 0, &sh) != kQOk)
+        {
+            atomicAdd(hard_fail, 1);
+            c = make_float4(0, 0, 0, 0);
+        }
+        out[k] = c;
+    }
+}
+
 // Pixel = sum of its output samples in sample order, times rcp(alpha); red
 // when empty (Reconstruction.cpp:665-719).
 __global__ void k_resolve(const float4* __restrict__ qcol, int M, float4* __restrict__ out, long long npix)
@@ -2217,9 +2355,6 @@ QParams make_params(const Ctx& c)
 
 int coop_blocks(const Ctx& c) { return c.num_sms * kCoopBlocksPerSM; }
 
-// overflow pass capacities
-constexpr int kOvStack = 512, kOvLeaf = 16384, kOvRs = 65536, kOvSurf = 4096;
-constexpr int kOvSlots = 4096;
 
 } // namespace
 
@@ -2979,6 +3114,84 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
         return TLFR_OVERFLOW;
     }
     return TLFR_OK;
+}
+
+
+// Shadow reconstruction of n queries (device, 8 floats each) into out (device).
+tlfr_status reconstruct_shadows(Ctx& c, const float* d_queries, int n, float4* d_out)
+{
+    cudaStream_t s = c.stream;
+    if (n <= 0)
+        return TLFR_OK;
+    if (!c.cur_records)
+    {
+        c.error = "no input records on the device";
+        return TLFR_BAD_ARG;
+    }
+    QParams P = make_params(c);
+    float2* wg = nullptr;
+    int* queue = nullptr;
+    CKQ(cudaMalloc(&wg, sizeof(float2) * (size_t)c.num_samples));
+    tlfr_status st = TLFR_OK;
+    if (cudaMalloc(&queue, sizeof(int) * (size_t)n) != cudaSuccess)
+    {
+        cudaFree(wg);
+        c.error = "shadow queue allocation failed";
+        return TLFR_OOM;
+    }
+    do
+    {
+        if (!c.d_stats && cudaMalloc(&c.d_stats, sizeof(DevStats) + 8 * sizeof(int)) != cudaSuccess)
+        {
+            st = TLFR_OOM;
+            break;
+        }
+        int* counters = reinterpret_cast<int*>(c.d_stats + 1);
+        cudaMemsetAsync(counters, 0, 8 * sizeof(int), s);
+        const int gb = (int)std::min<long long>(((long long)c.num_samples + 255) / 256, (long long)c.num_sms * 16);
+        TLFR_LAUNCH(c, k_gather_wg, gb > 0 ? gb : 1, 256, s, c.cur_records, c.s_id, c.num_samples, wg);
+        const int blocks = (int)std::min<long long>(((long long)n + kBlock - 1) / kBlock, (long long)c.num_sms * 16);
+        TLFR_LAUNCH(c, k_query_shadow, blocks, kBlock, s, P, d_queries, n, wg, d_out, queue, counters + 0, n);
+        int novf = 0, hard = 0;
+        cudaMemcpyAsync(&novf, counters + 0, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess)
+        {
+            st = TLFR_CUDA;
+            break;
+        }
+        if (novf > 0)
+        {
+            if (!c.ovf_scratch)
+            {
+                c.ovf_scratch_bytes = overflow_scratch_bytes();
+                if (cudaMalloc(&c.ovf_scratch, c.ovf_scratch_bytes) != cudaSuccess)
+                {
+                    st = TLFR_OOM;
+                    break;
+                }
+            }
+            const int slots = std::min(kOvSlots, novf);
+            TLFR_LAUNCH(c, k_query_shadow_large, (slots + 63) / 64, 64, s, P, d_queries, queue, counters + 0, n, wg,
+                        d_out, (char*)c.ovf_scratch, slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf), slots,
+                        counters + 1);
+            cudaMemcpyAsync(&hard, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+            if (cudaStreamSynchronize(s) != cudaSuccess)
+            {
+                st = TLFR_CUDA;
+                break;
+            }
+        }
+        if (hard > 0)
+        {
+            c.error = "a query exceeded the largest supported capacity";
+            st = TLFR_OVERFLOW;
+        }
+    } while (0);
+    if (st == TLFR_CUDA)
+        c.error = std::string("reconstruct_shadows: ") + cudaGetErrorString(cudaGetLastError());
+    cudaFree(wg);
+    cudaFree(queue);
+    return st;
 }
 
 tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h_trace, int stride)

@@ -108,6 +108,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_trace_queries": (ctypes.c_int, [_VP, _IP, ctypes.c_int, _FP, _IP, ctypes.c_int]),
         "tlfr_query_samples_noalloc": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
         "tlfr_output_sample_buffer": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+        "tlfr_reconstruct_shadows": (ctypes.c_int, [_VP, _FP, ctypes.c_int, _FP, _FP]),
         "tlfr_synth_scene": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_ulonglong, _FP, _FP]),
         "tlfr_synth_reference_image": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -349,6 +350,21 @@ class TreeGather:
         out = np.zeros((n, 5), np.float32)
         load_library().tlfr_output_samples(self._h, _f32p(out))
         return out
+
+    def reconstructShadows(self, queries: np.ndarray, density: Optional[np.ndarray] = None) -> np.ndarray:
+        """TreeGather::reconstructShadows (Reconstruction.cpp:302-344) for light-space query
+        records [..., 16]: per query the shadowed colour RGBA (the reference writes it into
+        the query buffer's sample colours)."""
+        q = np.ascontiguousarray(queries, np.float32).reshape(-1, 16)
+        n = q.shape[0]
+        out = np.zeros((n, 4), np.float32)
+        dp = None
+        if density is not None:
+            d = np.ascontiguousarray(density, np.float32).reshape(-1)
+            assert d.size == n
+            dp = _f32p(d)
+        _check(load_library().tlfr_reconstruct_shadows(self._h, _f32p(q), n, dp, _f32p(out)), self._h)
+        return out.reshape(tuple(np.shape(queries)[:-1]) + (4,))
 
     def output_sample_buffer(self) -> "UVTSampleBuffer":
         """The last reconstruction's output samples as a sample buffer (the reference's

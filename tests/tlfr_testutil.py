@@ -161,6 +161,16 @@ class CpuRecon:
             self.last_seconds = t
         return img
 
+    def shadows(self, queries, density):
+        """TreeGather::reconstructShadows of the reference build: queries [H, W, qspp, 16],
+        density [H, W, qspp]; returns the query buffer's colours [H, W, qspp, 4]."""
+        assert self.kind == "ref"
+        q = np.ascontiguousarray(queries, np.float32)
+        d = np.ascontiguousarray(density, np.float32)
+        out = np.zeros(q.shape[:3] + (4,), np.float32)
+        assert self.lib.ref_reconstruct_shadows(self.h, f32p(q), q.shape[2], f32p(d), f32p(out)) == 0
+        return out
+
     def gpu_toggle_image(self):
         """The reference's CPU restatement of its GPU-toggle algorithm over the whole
         image (CudaReconstruction::reconstructCPU, reference build only)."""
