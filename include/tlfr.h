@@ -215,6 +215,42 @@ tlfr_status tlfr_output_sample_buffer(tlfr_ctx* ctx, tlfr_buffer** out);
 tlfr_status tlfr_reconstruct_shadows(tlfr_ctx* ctx, const float* queries16, int num_queries, const float* density,
                                      float* rgba);
 
+/* A camera as the shadowed reconstruction reads it from CameraParams
+ * (CameraParams.hpp:74-141) and its CameraControls.  Matrices row-major,
+ * element (r, c) at [4*r + c], as the framework's Mat4f::get(r, c).         */
+typedef struct tlfr_view
+{
+    float projection[16];       /* CameraParams::projection                    */
+    float camera_to_world[16];  /* CameraParams::camera.getCameraToWorld()     */
+    float world_to_camera[16];  /* CameraParams::camera.getWorldToCamera()     */
+    float far_plane;            /* CameraParams::camera.getFar()               */
+    int   window_size[2];       /* CameraParams::windowSize                    */
+    float aperture_radius;      /* CameraParams::apertureRadius                */
+    float focus_distance;       /* CameraParams::focusDistance                 */
+} tlfr_view;
+
+/* Motion and defocus with soft shadows from a square area light,
+ * TreeGather::reconstructDofMotionShadows (Reconstruction.cpp:355-433, with
+ * FilterTask::process2, 723-829; the reference notes it is not callable from
+ * its application).  camera: the camera's context; light: a context over the
+ * light-space buffer of the same image size (its dw/dx, dw/dy in record fields
+ * 14-15); both with enable_cuda = 0.  Every output sample of the camera is
+ * reconstructed; its nearest sample, reprojected to the lens centre with the
+ * camera view's CoC, is mapped into the light's image; the light's hierarchy
+ * reconstructs it in shadow mode from a point on the light source (Sobol
+ * dimensions 3 and 4, rotated per pixel) with the dispersion scaled by
+ * sqrt(camera_density) of the nearest sample (the camera buffer's
+ * LIGHTSPACE_DENSITY channel, one float per input record in record order;
+ * NULL reads 1); the colour is lit by 1.5 * max(0, -L.N) with N rebuilt from
+ * the nearest sample's w gradients (lightSpaceDot, Util.cpp:201-224), plus
+ * 0.5 * ambient * the camera colour.  Samples beyond camera far - 0.01 or
+ * outside the light's image keep the camera colour; a pixel with an output
+ * sample the camera cannot reconstruct is red.  rgba: W*H*4 floats (device
+ * memory when rgba_on_device).  Synchronous.                                 */
+tlfr_status tlfr_reconstruct_dof_motion_shadows(tlfr_ctx* camera, const tlfr_view* camera_view,
+                                                const float* camera_density, tlfr_ctx* light,
+                                                const tlfr_view* light_view, float* rgba, int rgba_on_device);
+
 /* Run the output samples (x, y, i) listed in xyi[3*k ..] through the device query
  * path with tracing on.  rgba[4*k ..] = the query colour.  trace[k*trace_stride ..]:
  *   [0] flags: bit0 = 2R fetch, bit1 = widened beyond 2R, bit2 = surfaces merged,

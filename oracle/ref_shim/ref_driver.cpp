@@ -124,6 +124,84 @@ int ref_create(const float* records, int W, int H, int spp, float C0, float C1,
     }
 }
 
+// ref_create with the buffer's LIGHTSPACE_DENSITY channel (one float per record,
+// record order), which TreeGather reads into each sample's density
+// (Reconstruction.cpp:522, 547).
+int ref_create_density(const float* records, int W, int H, int spp, float C0, float C1, const float* density,
+                       float aperture, float focus, const float* uvt, int lensFilter, int timeFilter,
+                       void** out, double* build_seconds)
+{
+    RefHandle* h = new RefHandle();
+    try
+    {
+        h->sbuf = buffer_from_records(records, W, H, spp, C0, C1);
+        const int cid = h->sbuf->reserveChannel<float>("LIGHTSPACE_DENSITY");
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++)
+                for (int i = 0; i < spp; i++)
+                    (*(Array<float>*)(h->sbuf->m_channels[cid]))[h->sbuf->getIndex(x, y, i)] =
+                        density[((size_t)y * W + x) * spp + i];
+        return finish_create(h, aperture, focus, uvt, lensFilter, timeFilter, out, build_seconds);
+    }
+    catch (const std::exception& e)
+    {
+        g_error = e.what();
+        delete h->tg; delete h->params; delete h->sbuf; delete h;
+        return 1;
+    }
+}
+
+// The CameraParams fields the shadowed reconstruction reads (CameraParams.hpp:
+// 96-104): projection, the camera's matrices and far plane (row-major 4x4),
+// window size, aperture radius, focus distance.
+int ref_set_view(void* handle, const float* projection, const float* camera_to_world, const float* world_to_camera,
+                 float far_plane, int window_w, int window_h, float aperture_radius, float focus_distance)
+{
+    RefHandle* h = (RefHandle*)handle;
+    Mat4f P, C2W, W2C;
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++)
+        {
+            P(r, c) = projection[4 * r + c];
+            C2W(r, c) = camera_to_world[4 * r + c];
+            W2C(r, c) = world_to_camera[4 * r + c];
+        }
+    h->params->projection = P;
+    h->params->camera.setMatrices(C2W, W2C);
+    h->params->camera.setFar(far_plane);
+    h->params->windowSize = Vec2i(window_w, window_h);
+    h->params->apertureRadius = aperture_radius;
+    h->params->focusDistance = focus_distance;
+    return 0;
+}
+
+// TreeGather::reconstructDofMotionShadows (Reconstruction.cpp:355-433): camera
+// handle, light handle; rgba receives the W*H image.
+int ref_reconstruct_dof_motion_shadows(void* camera, void* light, float* rgba)
+{
+    RefHandle* c = (RefHandle*)camera;
+    RefHandle* l = (RefHandle*)light;
+    try
+    {
+        const int W = c->sbuf->getWidth(), H = c->sbuf->getHeight();
+        Image img(Vec2i(W, H));
+        c->tg->reconstructDofMotionShadows(img, *l->tg);
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++)
+            {
+                const Vec4f v = img.getVec4f(Vec2i(x, y));
+                float* o = rgba + ((size_t)y * W + x) * 4;
+                o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+            }
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_error = e.what();
+        return 1;
+    }
+}
+
 // Same, loading the buffer with the reference loader UVTSampleBuffer(const char*)
 // (SampleBuffer.cpp:230-387), which reads <path> and <path>.header.
 int ref_create_from_file(const char* path, float aperture, float focus, const float* uvt,

@@ -212,6 +212,25 @@ float sobol_dim3(int i)
     return (float)r * (1.0f / 4294967296.0f);
 }
 
+// Sobol dimension 4: primitive polynomial x^3 + x^2 + 1, initial direction
+// numbers m = (1, 1, 1).
+float sobol_dim4(int i)
+{
+    static uint32_t v[32];
+    static bool init = false;
+    if (!init)
+    {
+        v[0] = 1u << 31; v[1] = 1u << 30; v[2] = 1u << 29;
+        for (int k = 3; k < 32; k++)
+            v[k] = v[k - 1] ^ v[k - 3] ^ (v[k - 3] >> 3);
+        init = true;
+    }
+    uint32_t r = 0;
+    for (unsigned c = 0; i; i >>= 1, ++c)
+        if (i & 1) r ^= v[c];
+    return (float)r * (1.0f / 4294967296.0f);
+}
+
 void sobol_2d(int i, float* out)
 {
     uint32_t r1 = 0, r2 = 0;
@@ -440,6 +459,183 @@ tlfr_status run_build(tlfr_ctx* ctx, const float* d_rec)
     cudaEventElapsedTime(&ms, c.ev0, c.ev1);
     c.last.build_ms = ms;
     return TLFR_OK;
+}
+
+} // namespace
+
+namespace
+{
+
+// 4x4 float matrices with the framework's arithmetic (framework/base/Math.hpp):
+// products accumulate from 0 in index order; the inverse is the adjugate by
+// cofactors times rcp of the determinant summed along all four columns, times 4
+// (MatrixBase::inverted); 3x3 determinants by the rule of Sarrus in the
+// framework's term order (detImpl).
+struct Mat4
+{
+    float m[4][4];
+    Mat4()
+    {
+        for (int r = 0; r < 4; r++)
+            for (int c = 0; c < 4; c++)
+                m[r][c] = r == c ? 1.0f : 0.0f;
+    }
+    static Mat4 rows(const float* a)
+    {
+        Mat4 r;
+        for (int i = 0; i < 16; i++)
+            r.m[i / 4][i % 4] = a[i];
+        return r;
+    }
+    void store(float* a) const
+    {
+        for (int i = 0; i < 16; i++)
+            a[i] = m[i / 4][i % 4];
+    }
+};
+
+Mat4 operator*(const Mat4& a, const Mat4& b)
+{
+    Mat4 r;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+        {
+            float s = 0.0f;
+            for (int k = 0; k < 4; k++)
+                s += a.m[i][k] * b.m[k][j];
+            r.m[i][j] = s;
+        }
+    return r;
+}
+
+Mat4 operator-(const Mat4& a, const Mat4& b)
+{
+    Mat4 r;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+            r.m[i][j] = a.m[i][j] - b.m[i][j];
+    return r;
+}
+
+Mat4 transposed(const Mat4& a)
+{
+    Mat4 r;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+            r.m[i][j] = a.m[j][i];
+    return r;
+}
+
+float det3(const float s[3][3])
+{
+    return s[0][0] * s[1][1] * s[2][2] - s[0][0] * s[1][2] * s[2][1] +
+           s[1][0] * s[2][1] * s[0][2] - s[1][0] * s[2][2] * s[0][1] +
+           s[2][0] * s[0][1] * s[1][2] - s[2][0] * s[0][2] * s[1][1];
+}
+
+Mat4 inverted(const Mat4& a)
+{
+    Mat4 r;
+    float d = 0.0f;
+    float si = 1.0f;
+    for (int i = 0; i < 4; i++)
+    {
+        float sj = si;
+        for (int j = 0; j < 4; j++)
+        {
+            float sub[3][3];
+            for (int k = 0; k < 3; k++)
+                for (int l = 0; l < 3; l++)
+                    sub[k][l] = a.m[k < j ? k : k + 1][l < i ? l : l + 1];
+            const float dd = det3(sub) * sj;
+            r.m[i][j] = dd;
+            d += dd * a.m[j][i];
+            sj = -sj;
+        }
+        si = -si;
+    }
+    const float rd = tlfr::rcp(d);
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+            r.m[i][j] = (r.m[i][j] * rd) * 4.0f;
+    return r;
+}
+
+Mat4 scale3(float x, float y, float z)
+{
+    Mat4 r;
+    r.m[0][0] = x; r.m[1][1] = y; r.m[2][2] = z;
+    return r;
+}
+
+Mat4 translate3(float x, float y, float z)
+{
+    Mat4 r;
+    r.m[0][3] = x; r.m[1][3] = y; r.m[2][3] = z;
+    return r;
+}
+
+// CameraParams::getCocCoeffs (CameraParams.hpp:112-132): the projection of the
+// lens's half extent, scaled to the window width
+void view_coc(const tlfr_view& v, float coc[2])
+{
+    const Mat4 P = Mat4::rows(v.projection);
+    Mat4 dof;
+    const float ux = 0.5f, uy = 0.0f;
+    dof.m[0][2] = (ux * v.aperture_radius) / v.focus_distance;
+    dof.m[1][2] = (uy * v.aperture_radius) / v.focus_distance;
+    dof.m[2][2] = 1.0f;
+    dof.m[3][2] = 0.0f;
+    dof.m[0][3] = ux * v.aperture_radius;
+    dof.m[1][3] = uy * v.aperture_radius;
+    dof.m[2][3] = 0.0f;
+    dof.m[3][3] = 1.0f;
+    const Mat4 m = P * dof - P;
+    coc[0] = -m.m[0][3] * (float)v.window_size[0];
+    coc[1] = m.m[0][2] * (float)v.window_size[0];
+}
+
+// The matrices of TreeGather::reconstructDofMotionShadows (Reconstruction.cpp:365-392)
+// for an image of w x h pixels, and the light-source pattern of M output samples.
+void derive_dms_view(const tlfr_view& cam, const tlfr_view& light, int w, int h, int M, tlfr::DmsView& out)
+{
+    const Mat4 Pl = Mat4::rows(light.projection);
+    const Mat4 Pc = Mat4::rows(cam.projection);
+    const Mat4 invPc = inverted(Pc);
+    const Mat4 c2w = Mat4::rows(cam.camera_to_world);
+    const Mat4 lw2c = Mat4::rows(light.world_to_camera);
+    const Mat4 c2s = Pl * lw2c * c2w * invPc;
+    const Mat4 c2s2 = lw2c * c2w;
+    const Mat4 c2s2_inv_t = transposed(inverted(c2s2));
+    const Mat4 c2w_inv_t = transposed(inverted(c2w));
+    const Mat4 ws = scale3(0.5f * (float)w, 0.5f * (float)h, 0.5f) * translate3(1.0f, 1.0f, 1.0f);
+    const Mat4 invws = translate3(-1.0f, -1.0f, -1.0f) * scale3(2.f / (float)w, 2.f / (float)h, 2.f);
+    const Mat4 wsPc = ws * Pc;
+    Mat4 zfromw;
+    zfromw.m[2][2] = wsPc.m[2][3];
+    zfromw.m[2][3] = -wsPc.m[2][2];
+    const Mat4 c2l = ws * c2s * invws * zfromw;
+    (c2l).store(out.c2l);
+    (invws * zfromw).store(out.clip_xyw);
+    Mat4 ip = invPc;
+    for (int c = 0; c < 4; c++)
+    {
+        ip.m[2][c] = c == 2 ? -1.0f : 0.0f;
+        ip.m[3][c] = c == 3 ? 1.0f : 0.0f;
+    }
+    ip.store(out.ip);
+    (c2s2 * invPc).store(out.light_pos);
+    c2s2_inv_t.store(out.c2s_inv_t);
+    c2w_inv_t.store(out.c2w_inv_t);
+    out.cam_far_w = cam.far_plane - 1e-2f;
+    view_coc(cam, out.ccoc);
+    view_coc(light, out.lcoc);
+    out.light_uv.resize(2 * (size_t)M);
+    for (int i = 0; i < M; i++)
+    {
+        out.light_uv[2 * i + 0] = sobol_dim3(i + 1);
+        out.light_uv[2 * i + 1] = sobol_dim4(i + 1);
+    }
 }
 
 } // namespace
@@ -921,6 +1117,55 @@ int tlfr_output_samples(tlfr_ctx* ctx, float* out5)
 
 // TreeGather::reconstructShadows (Reconstruction.cpp:302-344) for a flat list of
 // light-space query samples.
+// Motion and defocus with soft shadows (TreeGather::reconstructDofMotionShadows,
+// Reconstruction.cpp:355-433).
+tlfr_status tlfr_reconstruct_dof_motion_shadows(tlfr_ctx* camera, const tlfr_view* camera_view,
+                                                const float* camera_density, tlfr_ctx* light,
+                                                const tlfr_view* light_view, float* rgba, int rgba_on_device)
+{
+    if (!camera || !light || !camera_view || !light_view || !rgba || camera == light)
+        return fail(camera, TLFR_BAD_ARG, "tlfr_reconstruct_dof_motion_shadows: bad argument");
+    tlfr::Ctx& c = camera->c;
+    tlfr::Ctx& l = light->c;
+    if (c.params.enable_cuda || l.params.enable_cuda)
+        return fail(camera, TLFR_BAD_ARG, "tlfr_reconstruct_dof_motion_shadows: the Filterer only (enable_cuda = 0)");
+    if (c.W != l.W || c.H != l.H)
+        return fail(camera, TLFR_BAD_ARG, "TreeGather::FilterTask::process2 -- cw!=lw || ch!=lh");
+    if (c.device != l.device)
+        return fail(camera, TLFR_BAD_ARG, "tlfr_reconstruct_dof_motion_shadows: contexts on different devices");
+    cudaSetDevice(c.device);
+    tlfr::DmsView v;
+    derive_dms_view(*camera_view, *light_view, c.W, c.H, c.out_spp, v);
+    const size_t npix = (size_t)c.W * c.H;
+    const size_t nrec = npix * (size_t)c.spp_in;
+    float* d_density = nullptr;
+    float4* d_img = rgba_on_device ? reinterpret_cast<float4*>(rgba) : nullptr;
+    tlfr_status st = TLFR_OK;
+    if (camera_density && cudaMalloc(&d_density, sizeof(float) * nrec) != cudaSuccess)
+        st = fail(camera, TLFR_OOM, "tlfr_reconstruct_dof_motion_shadows: allocation failed");
+    if (st == TLFR_OK && !d_img && cudaMalloc(&d_img, sizeof(float4) * npix) != cudaSuccess)
+        st = fail(camera, TLFR_OOM, "tlfr_reconstruct_dof_motion_shadows: allocation failed");
+    if (st == TLFR_OK && camera_density &&
+        cudaMemcpyAsync(d_density, camera_density, sizeof(float) * nrec, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+        st = fail(camera, TLFR_CUDA, "tlfr_reconstruct_dof_motion_shadows: upload failed");
+    if (st == TLFR_OK)
+    {
+        st = tlfr::reconstruct_dof_motion_shadows(c, l, v, d_density, d_img);
+        if (st != TLFR_OK)
+            st = fail(camera, st, "tlfr_reconstruct_dof_motion_shadows: %s", c.error.c_str());
+    }
+    if (st == TLFR_OK && !rgba_on_device)
+    {
+        if (cudaMemcpyAsync(rgba, d_img, sizeof(float4) * npix, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+            cudaStreamSynchronize(c.stream) != cudaSuccess)
+            st = fail(camera, TLFR_CUDA, "tlfr_reconstruct_dof_motion_shadows: download failed");
+    }
+    cudaFree(d_density);
+    if (!rgba_on_device)
+        cudaFree(d_img);
+    return st;
+}
+
 tlfr_status tlfr_reconstruct_shadows(tlfr_ctx* ctx, const float* queries16, int n, const float* density, float* rgba)
 {
     if (!ctx || n < 0 || (n > 0 && (!queries16 || !rgba)))

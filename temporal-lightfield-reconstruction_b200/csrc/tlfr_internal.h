@@ -256,6 +256,21 @@ size_t coop_scratch_bytes(int num_sms);
 tlfr_status trace_queries(Ctx& c, const int* h_xyi, int n, float* h_rgba, int* h_trace, int stride);
 // shadow reconstruction of n light-space queries (8 floats each, device) into d_out (device)
 tlfr_status reconstruct_shadows(Ctx& c, const float* d_queries, int n, float4* d_out);
+// Views of the shadowed reconstruction, derived on the host from the camera's
+// and the light's CameraParams (Reconstruction.cpp:365-392); matrices row-major.
+struct DmsView
+{
+    float c2l[16];          // ws * cameraToShadow * invws * cameraProjectedZfromW
+    float clip_xyw[16];     // invws * cameraProjectedZfromW
+    float ip[16];           // invCameraProjection with rows 2 and 3 replaced (Util.cpp:190-192)
+    float light_pos[16];    // cameraToShadow2 * invCameraProjection
+    float c2s_inv_t[16];    // cameraToShadow2 inverted, transposed
+    float c2w_inv_t[16];    // cameraToWorld inverted, transposed
+    float cam_far_w;        // camera far - 1e-2
+    float ccoc[2], lcoc[2]; // CameraParams::getCocCoeffs of the camera and the light
+    std::vector<float> light_uv;   // (sobol(3, i+1), sobol(4, i+1)) per output sample
+};
+tlfr_status reconstruct_dof_motion_shadows(Ctx& c, Ctx& l, const DmsView& v, const float* d_density, float4* d_img);
 // output samples through the full path with working storage in a fixed device array
 tlfr_status query_samples_noalloc(Ctx& c, const int* d_xyi, int n, float* d_rgba, int* d_overflow);
 // host-side output pattern (Reconstruction.cpp:452-512)

@@ -327,6 +327,15 @@ struct ShadowQ
 
 constexpr float kShadowBias = 0.01f;     // SHADOW_BIAS (RO.cpp:46)
 
+// The nearest sample of a reconstruction (Filterer::Result, RO.cpp:325-332):
+// its position reprojected to the output (u,v,t), its w at the output t and
+// its tree-ordered index (for its dw/dx, dw/dy and light-space density).
+struct QNear
+{
+    float x, y, w;
+    int index;
+};
+
 // w of sample i at time t (the ReconSample key of collectInputSamples2)
 TLFR_HD float sample_w_at(const QParams& P, int i, float t)
 {
@@ -344,7 +353,7 @@ TLFR_HD float sample_w_at(const QParams& P, int i, float t)
 // (0, 0, 0, alpha) where it is shadowed, no lens or time weights.
 template <bool TRACE>
 TLFR_HD int reconstruct_query(const QParams& P, Store& S, const Query& o, QStats& st, float4& out,
-                                 int* trace, int trace_cap, const ShadowQ* sh = nullptr)
+                                 int* trace, int trace_cap, const ShadowQ* sh = nullptr, QNear* nearp = nullptr)
 {
     float dispersion = sh ? sh->dispersion : P.disp0;
     int nsurf = 0;
@@ -507,6 +516,14 @@ TLFR_HD int reconstruct_query(const QParams& P, Store& S, const Query& o, QStats
         st.empty++;
         out = make_float4(0, 0, 0, 0);
         return kQOk;
+    }
+    if (nearp)
+    {
+        const RSample na = S.rs[S.surf[nearS].start + nearI];
+        nearp->x = na.x;
+        nearp->y = na.y;
+        nearp->w = sample_w_at(P, na.index, o.t);
+        nearp->index = na.index;
     }
     if (res.w == 0)
     {
@@ -2283,6 +2300,284 @@ k_query_shadow_large(QParams P, const float* __restrict__ queries, const int* __
     }
 }
 
+// ---------------------------------------------------------------------------
+// Motion and defocus with soft shadows from a square area light
+// (TreeGather::reconstructDofMotionShadows, R.cpp:355-433; FilterTask::process2,
+// R.cpp:723-829).  Every output sample is reconstructed from the camera's
+// hierarchy; the nearest sample's position and w place it in the light's
+// image through the camera-to-light matrix; a point on the light source
+// (Sobol dimensions 3 and 4 of the sample, rotated per pixel) moves it across
+// the light's lens; the light's hierarchy reconstructs it in shadow mode, and
+// the result is shaded with the normal rebuilt from the nearest sample's w
+// gradients (lightSpaceDot, viewSpaceNormalFromWGradients, Util.cpp:170-224).
+// The matrix and vector arithmetic keeps the framework's operation order
+// (framework/base/Math.hpp: sums accumulate from 0 in index order, rcp(0) = 0,
+// normalized = v * (1 * rcp(length))), so the results are bit-identical.
+// ---------------------------------------------------------------------------
+struct DmsParams
+{
+    float c2l[16];          // ws * cameraToShadow * invws * cameraProjectedZfromW (row-major)
+    float clip_xyw[16];     // invws * cameraProjectedZfromW
+    float ip[16];           // invCameraProjection, rows 2 and 3 = (0,0,-1,0), (0,0,0,1)
+    float light_pos[16];    // cameraToShadow2 * invCameraProjection
+    float c2s_inv_t[16];    // cameraToShadow2 inverted, transposed
+    float c2w_inv_t[16];    // cameraToWorld inverted, transposed
+    float cam_far_w;        // camera far - 1e-2
+    float ccoc0, ccoc1;     // CameraParams::getCocCoeffs of the camera
+    float lcoc0, lcoc1;     // and of the light
+    int   cw, ch;           // image size (the camera's and the light's)
+    const float2* light_uv; // (sobol(3, i+1), sobol(4, i+1)) per output sample i
+    const float2* cam_wg;   // dw/dx, dw/dy per camera tree-ordered sample
+    const float*  cam_density;   // light-space density per camera tree-ordered sample (null: 1)
+    const float2* light_wg; // dw/dx, dw/dy per light tree-ordered sample
+};
+
+// Mat4f * Vec4f (Math.hpp:1000-1011)
+TLFR_HD float4 m4_apply(const float* m, float4 v)
+{
+    float r[4];
+    for (int i = 0; i < 4; i++)
+    {
+        float a = 0.0f;
+        a += m[4 * i + 0] * v.x;
+        a += m[4 * i + 1] * v.y;
+        a += m[4 * i + 2] * v.z;
+        a += m[4 * i + 3] * v.w;
+        r[i] = a;
+    }
+    return make_float4(r[0], r[1], r[2], r[3]);
+}
+
+TLFR_HD float3 v3_normalized(float3 v)
+{
+    float l2 = 0.0f;
+    l2 += v.x * v.x;
+    l2 += v.y * v.y;
+    l2 += v.z * v.z;
+    const float k = 1.0f * rcp(sqrtf(l2));
+    return make_float3(v.x * k, v.y * k, v.z * k);
+}
+
+TLFR_HD float v3_dot(float3 a, float3 b)
+{
+    float r = 0.0f;
+    r += a.x * b.x;
+    r += a.y * b.y;
+    r += a.z * b.z;
+    return r;
+}
+
+// The light-source offset of pixel (x, y): the framework's Random seeded with
+// hashBits(x, y) (Ranrot-A, framework/base/Random.cpp), two draws.  The
+// reference builds the offset as Vec2f(random.getF32(), random.getF32()), whose
+// arguments its compilers evaluate right to left: x takes the second draw.
+TLFR_HD void light_uv_offset(int x, int y, float& ou, float& ov)
+{
+    uint32_t seed = hash_bits((uint32_t)x, (uint32_t)y);
+    uint32_t buf[11];
+    if (seed == 0)
+        seed--;
+    for (int k = 0; k < 11; k++)
+    {
+        seed ^= seed << 13;
+        seed ^= seed >> 17;
+        seed ^= seed << 5;
+        buf[k] = seed;
+    }
+    int p1 = 0, p2 = 7;
+    uint32_t draw = 0;
+    for (int k = 0; k < 13; k++)
+    {
+        uint32_t v = buf[p1] + buf[p2];
+        v = (v << 13) | (v >> 19);
+        buf[p1] = v;
+        p1--; p1 += (p1 >> 31) & 11;
+        p2--; p2 += (p2 >> 31) & 11;
+        if (k == 11)
+            draw = v;
+        if (k == 12)
+        {
+            ou = (float)v * (1.0f / 4294967296.0f);
+            ov = (float)draw * (1.0f / 4294967296.0f);
+        }
+    }
+}
+
+// Output sample i of pixel (x, y).  red: the camera reconstruction found
+// nothing, which turns the whole pixel red (R.cpp:764-768).
+TLFR_HD int dms_sample(const QParams& Pc, const QParams& Pl, const DmsParams& D, Store& S, int x, int y, int i,
+                       float4& col, bool& red, QStats& st)
+{
+    const Query o = make_query(Pc, x, y, i);
+    QNear nr{ 0.0f, 0.0f, 0.0f, 0 };
+    float4 cc;
+    if (reconstruct_query<false>(Pc, S, o, st, cc, nullptr, 0, nullptr, &nr) != kQOk)
+        return kQOverflow;
+    red = cc.x == 0.0f && cc.y == 0.0f && cc.z == 0.0f && cc.w == 0.0f;
+    col = cc;
+    if (red || !(nr.w <= D.cam_far_w))
+        return kQOk;
+
+    // Sample::reprojectToUVCenter (Reconstruction.hpp:93-97) with the camera's CoC
+    const float cr = D.ccoc0 / nr.w + D.ccoc1;
+    const float sx = nr.x - o.u * cr, sy = nr.y - o.v * cr;
+    const float4 xyw = make_float4(sx * nr.w, sy * nr.w, 1.0f, nr.w);
+    float4 lp = m4_apply(D.c2l, xyw);
+    const float lc = rcp(lp.w);
+    lp.x *= lc; lp.y *= lc; lp.z *= lc;
+    if (!(lp.x >= 0.0f && lp.y >= 0.0f && lp.x <= (float)D.cw && lp.y <= (float)D.ch && lp.w > 0.0f))
+        return kQOk;
+
+    // the light-space query: a point on the square light source [-1,1]^2
+    float ou = 0.0f, ov = 0.0f;
+    light_uv_offset(x, y, ou, ov);
+    const float2 s34 = D.light_uv[i];
+    float u = s34.x + ou, v = s34.y + ov;
+    if (u >= 1.0f) u -= 1.0f;
+    if (v >= 1.0f) v -= 1.0f;
+    Query ls;
+    ls.u = 2.0f * u - 1.0f;
+    ls.v = 2.0f * v - 1.0f;
+    ls.t = o.t;
+    const float lr = D.lcoc0 / lp.w + D.lcoc1;
+    ls.x = lp.x + ls.u * lr;
+    ls.y = lp.y + ls.v * lr;
+    const float density = D.cam_density ? D.cam_density[nr.index] : 1.0f;
+    const ShadowQ sh{ lp.w, Pl.disp0 * sqrtf(density), D.light_wg };
+    float4 sc;
+    if (reconstruct_query<false>(Pl, S, ls, st, sc, nullptr, 0, &sh) != kQOk)
+        return kQOverflow;
+
+    // lightSpaceDot: the view-space normal from the w gradients, against the
+    // direction to the light
+    const float4 p = m4_apply(D.clip_xyw, xyw);
+    const float pu = p.x / p.w, pv = p.y / p.w;
+    const float2 g = D.cam_wg[nr.index];
+    const float dwdu = g.x * ((float)D.cw / 2.0f);
+    const float dwdv = g.y * ((float)D.ch / 2.0f);
+    const float4 b1 = m4_apply(D.ip, make_float4(p.w + pu * dwdu, pv * dwdu, dwdu, 0.0f));
+    const float4 b2 = m4_apply(D.ip, make_float4(pu * dwdv, p.w + pv * dwdv, dwdv, 0.0f));
+    const float3 n = v3_normalized(make_float3(b1.y * b2.z - b1.z * b2.y, b1.z * b2.x - b1.x * b2.z,
+                                               b1.x * b2.y - b1.y * b2.x));
+    const float4 nl = m4_apply(D.c2s_inv_t, make_float4(n.x, n.y, n.z, 0.0f));
+    const float4 pl = m4_apply(D.light_pos, p);
+    const float plc = rcp(pl.w);
+    const float ldotn = -v3_dot(v3_normalized(make_float3(pl.x * plc, pl.y * plc, pl.z * plc)),
+                                v3_normalized(make_float3(nl.x, nl.y, nl.z)));
+    const float4 wn = m4_apply(D.c2w_inv_t, make_float4(n.x, n.y, n.z, 0.0f));
+    const float ambient = wn.y * 0.5f + 0.5f;
+    const float k = maxr(ldotn, 0.0f) * 1.5f;     // LIGHTING_SCALE (R.cpp:34)
+    const float a = ambient * 0.5f;               // AMBIENT_SCALE (R.cpp:35)
+    col = make_float4(sc.x * k + cc.x * a, sc.y * k + cc.y * a, sc.z * k + cc.z * a, 1.0f);
+    return kQOk;
+}
+
+// dw/dx, dw/dy and the light-space density of every tree-ordered sample (density null: skipped)
+__global__ void k_gather_wg_density(const float* __restrict__ records, const int* __restrict__ s_id, int n,
+                                    const float* __restrict__ density_in, float2* __restrict__ wg,
+                                    float* __restrict__ density)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    {
+        const int id = s_id[k];
+        const float* r = records + (size_t)id * 16;
+        wg[k] = make_float2(r[14], r[15]);
+        if (density_in)
+            density[k] = density_in[id];
+    }
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_query_dms(QParams Pc, QParams Pl, DmsParams D, float4* __restrict__ qcol, int* __restrict__ red,
+            int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap)
+{
+    int stack[kStackCap];
+    Leaf leaves[kLeafCap];
+    RSample rs[kRsCap];
+    Surf surf[kSurfCap];
+    Store S{ stack, kStackCap, leaves, kLeafCap, rs, kRsCap, surf, kSurfCap };
+    const long long n = (long long)Pc.W * Pc.H * Pc.M;
+    for (long long q = blockIdx.x * (long long)kBlock + threadIdx.x; q < n; q += (long long)gridDim.x * kBlock)
+    {
+        const int pix = (int)(q / Pc.M), i = (int)(q % Pc.M);
+        QStats qs{};
+        float4 c;
+        bool r = false;
+        if (dms_sample(Pc, Pl, D, S, pix % Pc.W, pix / Pc.W, i, c, r, qs) == kQOk)
+        {
+            qcol[q] = c;
+            if (r)
+                red[pix] = 1;
+        }
+        else
+        {
+            const int slot = atomicAdd(ovf_count, 1);
+            if (slot < ovf_cap)
+                ovf_queue[slot] = (int)q;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(64)
+k_query_dms_large(QParams Pc, QParams Pl, DmsParams D, const int* __restrict__ queue, const int* __restrict__ count_ptr,
+                  int cap, float4* __restrict__ qcol, int* __restrict__ red, char* arena, size_t slot_bytes,
+                  int num_slots, int* hard_fail)
+{
+    const int count = min(*count_ptr, cap);
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= num_slots)
+        return;
+    char* base = arena + (size_t)slot * slot_bytes;
+    Store S;
+    S.stack = (int*)base;                      S.stack_cap = kOvStack;
+    S.leaves = (Leaf*)(S.stack + kOvStack);    S.leaf_cap = kOvLeaf;
+    S.rs = (RSample*)(S.leaves + kOvLeaf);     S.rs_cap = kOvRs;
+    S.surf = (Surf*)(S.rs + kOvRs);            S.surf_cap = kOvSurf;
+    for (int j = slot; j < count; j += num_slots)
+    {
+        const int q = queue[j];
+        const int pix = q / Pc.M, i = q % Pc.M;
+        QStats qs{};
+        float4 c;
+        bool r = false;
+        if (dms_sample(Pc, Pl, D, S, pix % Pc.W, pix / Pc.W, i, c, r, qs) != kQOk)
+        {
+            atomicAdd(hard_fail, 1);
+            c = make_float4(0, 0, 0, 0);
+        }
+        qcol[q] = c;
+        if (r)
+            red[pix] = 1;
+    }
+}
+
+// Pixel of the shadowed reconstruction: red when one of its output samples
+// found nothing in the camera's hierarchy, else the sum of its samples in
+// order times rcp(alpha), red when alpha is 0 (R.cpp:764-768, 823-828).
+__global__ void k_resolve_dms(const float4* __restrict__ qcol, const int* __restrict__ red, int M,
+                              float4* __restrict__ out, long long npix)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x)
+    {
+        float4 s = make_float4(0, 0, 0, 0);
+        if (red[p])
+            s = make_float4(1, 0, 0, 1);
+        else
+        {
+            const float4* c = qcol + p * M;
+            for (int i = 0; i < M; i++)
+            {
+                const float4 v = c[i];
+                s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+            }
+            if (s.w == 0)
+                s = make_float4(1, 0, 0, 1);
+        }
+        const float r = rcp(s.w);
+        out[p] = make_float4(s.x * r, s.y * r, s.z * r, s.w * r);
+    }
+}
+
 // Pixel = sum of its output samples in sample order, times rcp(alpha); red
 // when empty (Reconstruction.cpp:665-719).
 __global__ void k_resolve(const float4* __restrict__ qcol, int M, float4* __restrict__ out, long long npix)
@@ -2960,20 +3255,13 @@ static tlfr_status reconstruct_toggle(Ctx& c, float4* d_rgba)
     return TLFR_OK;
 }
 
-tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
+// Output-sample colours, the full-path and overflow queues of a frame of nq
+// output samples, and the statistics block.  The overflow queue holds every
+// output sample in the worst case, so no scene can exceed it.
+tlfr_status frame_buffers(Ctx& c, long long nq)
 {
-    cudaStream_t s = c.stream;
-    const long long npix = (long long)c.W * c.H;
-    const long long nq = npix * c.out_spp;
-    if (nq >= kQueueRestart)
-    {
-        c.error = "more than 2^30 output samples in one frame";
-        return TLFR_BAD_ARG;
-    }
     if ((size_t)nq > c.qcol_cap)
     {
-        // the overflow queue holds every output sample in the worst case, so no
-        // scene can exceed it
         cudaFree(c.qcol); cudaFree(c.heavy_queue); cudaFree(c.ovf_queue);
         c.qcol = nullptr; c.heavy_queue = nullptr; c.ovf_queue = nullptr; c.qcol_cap = 0; c.ovf_cap = 0;
         CKQ(cudaMalloc(&c.qcol, sizeof(float4) * nq));
@@ -2984,6 +3272,22 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
     }
     if (!c.d_stats)
         CKQ(cudaMalloc(&c.d_stats, sizeof(DevStats) + 8 * sizeof(int)));
+    return TLFR_OK;
+}
+
+tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
+{
+    cudaStream_t s = c.stream;
+    const long long npix = (long long)c.W * c.H;
+    const long long nq = npix * c.out_spp;
+    if (nq >= kQueueRestart)
+    {
+        c.error = "more than 2^30 output samples in one frame";
+        return TLFR_BAD_ARG;
+    }
+    tlfr_status fb = frame_buffers(c, nq);
+    if (fb != TLFR_OK)
+        return fb;
     if (c.params.enable_cuda)
         return reconstruct_toggle(c, d_rgba);
     int* counters = reinterpret_cast<int*>(c.d_stats + 1);   // [0] overflow, [1] hard, [2] heavy
@@ -3191,6 +3495,135 @@ tlfr_status reconstruct_shadows(Ctx& c, const float* d_queries, int n, float4* d
         c.error = std::string("reconstruct_shadows: ") + cudaGetErrorString(cudaGetLastError());
     cudaFree(wg);
     cudaFree(queue);
+    return st;
+}
+
+// Motion and defocus with soft shadows (TreeGather::reconstructDofMotionShadows,
+// Reconstruction.cpp:355-433): camera context c, light context l (same image
+// size), derived views v, the camera buffer's light-space density per input
+// record (device, or null), the image into d_img (device).
+tlfr_status reconstruct_dof_motion_shadows(Ctx& c, Ctx& l, const DmsView& v, const float* d_density,
+                                           float4* d_img)
+{
+    cudaStream_t s = c.stream;
+    if (!c.cur_records || !l.cur_records)
+    {
+        c.error = "no input records on the device";
+        return TLFR_BAD_ARG;
+    }
+    const long long npix = (long long)c.W * c.H;
+    const long long nq = npix * c.out_spp;
+    if (nq >= kQueueRestart)
+    {
+        c.error = "more than 2^30 output samples in one frame";
+        return TLFR_BAD_ARG;
+    }
+    if ((int)v.light_uv.size() != 2 * c.out_spp)
+    {
+        c.error = "light-source pattern size mismatch";
+        return TLFR_BAD_ARG;
+    }
+    tlfr_status st = frame_buffers(c, nq);
+    if (st != TLFR_OK)
+        return st;
+    // the light's hierarchy was built on the light context's own stream
+    if (cudaStreamSynchronize(l.stream) != cudaSuccess)
+    {
+        c.error = std::string("light context: ") + cudaGetErrorString(cudaGetLastError());
+        return TLFR_CUDA;
+    }
+    float2* cam_wg = nullptr;
+    float2* light_wg = nullptr;
+    float* cam_density = nullptr;
+    float2* light_uv = nullptr;
+    int* red = nullptr;
+    auto release = [&]() { cudaFree(cam_wg); cudaFree(light_wg); cudaFree(cam_density); cudaFree(light_uv); cudaFree(red); };
+    if (cudaMalloc(&cam_wg, sizeof(float2) * (size_t)std::max(1, c.num_samples)) != cudaSuccess ||
+        cudaMalloc(&light_wg, sizeof(float2) * (size_t)std::max(1, l.num_samples)) != cudaSuccess ||
+        (d_density && cudaMalloc(&cam_density, sizeof(float) * (size_t)std::max(1, c.num_samples)) != cudaSuccess) ||
+        cudaMalloc(&light_uv, sizeof(float2) * (size_t)c.out_spp) != cudaSuccess ||
+        cudaMalloc(&red, sizeof(int) * (size_t)npix) != cudaSuccess)
+    {
+        release();
+        c.error = "shadow reconstruction: allocation failed";
+        return TLFR_OOM;
+    }
+    DmsParams D;
+    memcpy(D.c2l, v.c2l, sizeof(D.c2l));
+    memcpy(D.clip_xyw, v.clip_xyw, sizeof(D.clip_xyw));
+    memcpy(D.ip, v.ip, sizeof(D.ip));
+    memcpy(D.light_pos, v.light_pos, sizeof(D.light_pos));
+    memcpy(D.c2s_inv_t, v.c2s_inv_t, sizeof(D.c2s_inv_t));
+    memcpy(D.c2w_inv_t, v.c2w_inv_t, sizeof(D.c2w_inv_t));
+    D.cam_far_w = v.cam_far_w;
+    D.ccoc0 = v.ccoc[0]; D.ccoc1 = v.ccoc[1];
+    D.lcoc0 = v.lcoc[0]; D.lcoc1 = v.lcoc[1];
+    D.cw = c.W; D.ch = c.H;
+    D.light_uv = light_uv;
+    D.cam_wg = cam_wg;
+    D.cam_density = cam_density;
+    D.light_wg = light_wg;
+    const QParams Pc = make_params(c);
+    const QParams Pl = make_params(l);
+    int* counters = reinterpret_cast<int*>(c.d_stats + 1);
+    do
+    {
+        cudaMemcpyAsync(light_uv, v.light_uv.data(), sizeof(float2) * (size_t)c.out_spp, cudaMemcpyHostToDevice, s);
+        cudaMemsetAsync(red, 0, sizeof(int) * (size_t)npix, s);
+        cudaMemsetAsync(counters, 0, 8 * sizeof(int), s);
+        const int gc = (int)std::min<long long>(((long long)c.num_samples + 255) / 256, (long long)c.num_sms * 16);
+        TLFR_LAUNCH(c, k_gather_wg_density, gc > 0 ? gc : 1, 256, s, c.cur_records, c.s_id, c.num_samples, d_density,
+                    cam_wg, cam_density);
+        const int gl = (int)std::min<long long>(((long long)l.num_samples + 255) / 256, (long long)c.num_sms * 16);
+        TLFR_LAUNCH(c, k_gather_wg_density, gl > 0 ? gl : 1, 256, s, l.cur_records, l.s_id, l.num_samples, nullptr,
+                    light_wg, nullptr);
+        const int blocks = (int)std::min<long long>((nq + kBlock - 1) / kBlock, (long long)c.num_sms * 16);
+        TLFR_LAUNCH(c, k_query_dms, blocks, kBlock, s, Pc, Pl, D, c.qcol, red, c.ovf_queue, counters + 0,
+                    (int)c.ovf_cap);
+        int novf = 0, hard = 0;
+        cudaMemcpyAsync(&novf, counters + 0, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess)
+        {
+            st = TLFR_CUDA;
+            break;
+        }
+        if (novf > 0)
+        {
+            if (!c.ovf_scratch)
+            {
+                c.ovf_scratch_bytes = overflow_scratch_bytes();
+                if (cudaMalloc(&c.ovf_scratch, c.ovf_scratch_bytes) != cudaSuccess)
+                {
+                    c.error = "shadow reconstruction: allocation failed";
+                    st = TLFR_OOM;
+                    break;
+                }
+            }
+            const int slots = std::min(kOvSlots, novf);
+            TLFR_LAUNCH(c, k_query_dms_large, (slots + 63) / 64, 64, s, Pc, Pl, D, c.ovf_queue, counters + 0,
+                        (int)c.ovf_cap, c.qcol, red, (char*)c.ovf_scratch,
+                        slot_bytes_for(kOvStack, kOvLeaf, kOvRs, kOvSurf), slots, counters + 1);
+            cudaMemcpyAsync(&hard, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+            if (cudaStreamSynchronize(s) != cudaSuccess)
+            {
+                st = TLFR_CUDA;
+                break;
+            }
+        }
+        if (hard > 0)
+        {
+            c.error = "an output sample exceeded the largest supported capacity";
+            st = TLFR_OVERFLOW;
+            break;
+        }
+        const int rb = (int)std::min<long long>((npix + 255) / 256, (long long)c.num_sms * 16);
+        TLFR_LAUNCH(c, k_resolve_dms, rb > 0 ? rb : 1, 256, s, c.qcol, red, c.out_spp, d_img, npix);
+        if (cudaStreamSynchronize(s) != cudaSuccess)
+            st = TLFR_CUDA;
+    } while (0);
+    if (st == TLFR_CUDA)
+        c.error = std::string("reconstruct_dof_motion_shadows: ") + cudaGetErrorString(cudaGetLastError());
+    release();
     return st;
 }
 

@@ -109,6 +109,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "tlfr_query_samples_noalloc": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
         "tlfr_output_sample_buffer": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
         "tlfr_reconstruct_shadows": (ctypes.c_int, [_VP, _FP, ctypes.c_int, _FP, _FP]),
+        "tlfr_reconstruct_dof_motion_shadows": (ctypes.c_int, [_VP, ctypes.POINTER(_View), _FP, _VP,
+                                                               ctypes.POINTER(_View), _FP, ctypes.c_int]),
         "tlfr_synth_scene": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_ulonglong, _FP, _FP]),
         "tlfr_synth_reference_image": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -234,6 +236,17 @@ class UVTSampleBuffer:
             self._h = None
 
 
+class _View(ctypes.Structure):
+    _fields_ = [("projection", ctypes.c_float * 16), ("camera_to_world", ctypes.c_float * 16),
+                ("world_to_camera", ctypes.c_float * 16), ("far_plane", ctypes.c_float),
+                ("window_size", ctypes.c_int * 2), ("aperture_radius", ctypes.c_float),
+                ("focus_distance", ctypes.c_float)]
+
+
+def _identity():
+    return np.eye(4, dtype=np.float32)
+
+
 @dataclass
 class CameraParams:
     """The CameraParams fields the reconstruction path reads (CameraParams.hpp:74-107).
@@ -251,6 +264,27 @@ class CameraParams:
     enableCuda: bool = False
     outputSpp: int = 0          # 0: reference default (128, or 1 with overrideUVT)
     device: int = 0
+    # the camera, read only by the shadowed reconstruction (CameraParams.hpp:96-104;
+    # CameraControls getCameraToWorld / getWorldToCamera / getFar): 4x4 matrices
+    projection: np.ndarray = field(default_factory=_identity)
+    cameraToWorld: np.ndarray = field(default_factory=_identity)
+    worldToCamera: np.ndarray = field(default_factory=_identity)
+    far: float = 3.0
+    windowSize: Tuple[int, int] = (0, 0)
+    apertureRadius: float = 0.0
+    focusDistance: float = 1.0
+
+    def _view(self) -> _View:
+        v = _View()
+        for name, m in (("projection", self.projection), ("camera_to_world", self.cameraToWorld),
+                        ("world_to_camera", self.worldToCamera)):
+            a = np.ascontiguousarray(m, np.float32).reshape(16)
+            getattr(v, name)[:] = [float(x) for x in a]
+        v.far_plane = self.far
+        v.window_size[0], v.window_size[1] = int(self.windowSize[0]), int(self.windowSize[1])
+        v.aperture_radius = self.apertureRadius
+        v.focus_distance = self.focusDistance
+        return v
 
     def _to_c(self, aperture: float, focus: float) -> _Params:
         p = _Params()
@@ -365,6 +399,24 @@ class TreeGather:
             dp = _f32p(d)
         _check(load_library().tlfr_reconstruct_shadows(self._h, _f32p(q), n, dp, _f32p(out)), self._h)
         return out.reshape(tuple(np.shape(queries)[:-1]) + (4,))
+
+    def reconstructDofMotionShadows(self, shadowTG: "TreeGather",
+                                    density: Optional[np.ndarray] = None) -> np.ndarray:
+        """TreeGather::reconstructDofMotionShadows (Reconstruction.cpp:355-433): this
+        hierarchy is the camera's, shadowTG's the light's (same image size); the views come
+        from the two TreeGathers' CameraParams.  density: the camera buffer's
+        LIGHTSPACE_DENSITY channel, one float per input record ([H, W, spp] or flat), or None
+        for 1.  Returns the image [H, W, 4]."""
+        W, H = self.size
+        out = np.zeros((H, W, 4), np.float32)
+        dp = None
+        if density is not None:
+            d = np.ascontiguousarray(density, np.float32).reshape(-1)
+            dp = _f32p(d)
+        cv, lv = self.params._view(), shadowTG.params._view()
+        _check(load_library().tlfr_reconstruct_dof_motion_shadows(self._h, ctypes.byref(cv), dp, shadowTG._h,
+                                                                   ctypes.byref(lv), _f32p(out), 0), self._h)
+        return out
 
     def output_sample_buffer(self) -> "UVTSampleBuffer":
         """The last reconstruction's output samples as a sample buffer (the reference's

@@ -41,3 +41,68 @@ def test_gpu_shadows_match_reference(preset, W, H, spp, qspp, seed):
     # the queries behind the surface are (partly) shadowed, the ones in front lit
     lum = got[..., :3].sum(-1)
     assert (lum == 0).any() and (lum > 0).any()
+
+
+def _perspective(fov_deg, aspect, near, far):
+    f = 1.0 / np.tan(np.radians(fov_deg) / 2)
+    return np.array([[f / aspect, 0, 0, 0],
+                     [0, f, 0, 0],
+                     [0, 0, (far + near) / (near - far), 2 * far * near / (near - far)],
+                     [0, 0, -1, 0]], np.float64)
+
+
+def _pose(yaw_deg, t):
+    a = np.radians(yaw_deg)
+    m = np.eye(4)
+    m[0, 0], m[0, 2], m[2, 0], m[2, 2] = np.cos(a), np.sin(a), -np.sin(a), np.cos(a)
+    m[:3, 3] = t
+    return m
+
+
+def _dms_scene(W, H, spp, seed, cam_far, light_offset, density):
+    """A camera buffer and a light-space buffer of the same size (the planes scene, w in
+    2..12, with random depth gradients), the two cameras (the light shifted and turned),
+    and the camera buffer's light-space density channel (or None)."""
+    rng = np.random.default_rng(seed)
+    cam_rec, cam_coc = tlfr.synth_scene(tlfr.SCENE_PLANES, W, H, spp, seed)
+    light_rec, light_coc = tlfr.synth_scene(tlfr.SCENE_PLANES, W, H, spp, seed + 1)
+    for r in (cam_rec, light_rec):
+        r[..., 14:16] = rng.uniform(-0.04, 0.04, r.shape[:3] + (2,)).astype(np.float32)
+    proj = _perspective(60.0, W / H, 0.1, 100.0).astype(np.float32)
+    c2w = _pose(0.0, (0.0, 0.0, 0.0))
+    l2w = _pose(8.0, light_offset)
+    cam = tlfr.CameraParams(projection=proj, cameraToWorld=c2w.astype(np.float32),
+                            worldToCamera=np.linalg.inv(c2w).astype(np.float32), far=cam_far,
+                            windowSize=(W, H), apertureRadius=0.05, focusDistance=5.0)
+    light = tlfr.CameraParams(projection=proj, cameraToWorld=l2w.astype(np.float32),
+                              worldToCamera=np.linalg.inv(l2w).astype(np.float32), far=100.0,
+                              windowSize=(W, H), apertureRadius=0.5, focusDistance=5.0)
+    dens = rng.uniform(0.5, 2.0, cam_rec.shape[:3]).astype(np.float32) if density else None
+    return cam_rec, cam_coc, cam, light_rec, light_coc, light, dens
+
+
+_dms_scene.cases = [
+    (40, 24, 4, 93, 100.0, (0.3, 0.2, 0.0), True),
+    (48, 32, 8, 94, 7.0, (-0.5, 0.1, 0.3), False),
+]
+
+
+@pytest.mark.parametrize("case", _dms_scene.cases)
+def test_gpu_dof_motion_shadows_match_reference(case):
+    """TreeGather::reconstructDofMotionShadows (Reconstruction.cpp:355-433, 723-829) on the
+    GPU against the reference build's, every pixel bit for bit."""
+    if not ref_available():
+        pytest.skip("reference build absent")
+    cam_rec, cam_coc, cam, light_rec, light_coc, light, dens = _dms_scene(*case)
+    cg = tlfr.TreeGather(tlfr.UVTSampleBuffer(records=cam_rec, coc=cam_coc), cam)
+    lg = tlfr.TreeGather(tlfr.UVTSampleBuffer(records=light_rec, coc=light_coc), light)
+    got = cg.reconstructDofMotionShadows(lg, dens)
+    c = CpuRecon("ref", cam_rec, cam_coc, density=dens)
+    l = CpuRecon("ref", light_rec, light_coc)
+    c.set_view(cam)
+    l.set_view(light)
+    want = c.dof_motion_shadows(l)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    # the shading changed the camera's image
+    plain = cg.reconstructDofMotion()
+    assert (np.abs(got - plain).max(-1) > 1e-3).mean() > 0.2

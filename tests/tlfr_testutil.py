@@ -65,7 +65,7 @@ class CpuRecon:
     """Common handle over the oracle restatement ('orc') or the reference build ('ref')."""
 
     def __init__(self, kind, records, coc, aperture=1.0, focus=1.0, uvt=None, lens=0, time=0,
-                 output_spp=0, nthreads=8, m64=False):
+                 output_spp=0, nthreads=8, m64=False, density=None):
         self.kind = kind
         rec = np.ascontiguousarray(records, np.float32)
         H, W, S = rec.shape[:3]
@@ -83,9 +83,16 @@ class CpuRecon:
         else:
             self.lib = ref_lib(m64)
             os.environ.setdefault("TLFR_REF_THREADS", str(nthreads))
-            r = self.lib.ref_create(f32p(rec), W, H, S, ctypes.c_float(coc[0]), ctypes.c_float(coc[1]),
-                                    ctypes.c_float(aperture), ctypes.c_float(focus), uv, lens, time,
-                                    ctypes.byref(h), ctypes.byref(bs))
+            if density is None:
+                r = self.lib.ref_create(f32p(rec), W, H, S, ctypes.c_float(coc[0]), ctypes.c_float(coc[1]),
+                                        ctypes.c_float(aperture), ctypes.c_float(focus), uv, lens, time,
+                                        ctypes.byref(h), ctypes.byref(bs))
+            else:
+                self._density = np.ascontiguousarray(density, np.float32)
+                r = self.lib.ref_create_density(f32p(rec), W, H, S, ctypes.c_float(coc[0]),
+                                                ctypes.c_float(coc[1]), f32p(self._density), ctypes.c_float(aperture),
+                                                ctypes.c_float(focus), uv, lens, time, ctypes.byref(h),
+                                                ctypes.byref(bs))
             if r:
                 self.lib.ref_last_error.restype = ctypes.c_char_p
                 raise RuntimeError(self.lib.ref_last_error())
@@ -160,6 +167,24 @@ class CpuRecon:
                 t += self.last_seconds
             self.last_seconds = t
         return img
+
+    def set_view(self, params):
+        """The camera fields of a tlfr.CameraParams into the reference's CameraParams."""
+        assert self.kind == "ref"
+        m = [np.ascontiguousarray(x, np.float32).reshape(16) for x in
+             (params.projection, params.cameraToWorld, params.worldToCamera)]
+        assert self.lib.ref_set_view(self.h, f32p(m[0]), f32p(m[1]), f32p(m[2]), ctypes.c_float(params.far),
+                                     int(params.windowSize[0]), int(params.windowSize[1]),
+                                     ctypes.c_float(params.apertureRadius), ctypes.c_float(params.focusDistance)) == 0
+        self._views = m
+
+    def dof_motion_shadows(self, light):
+        """TreeGather::reconstructDofMotionShadows of the reference build: this handle is the
+        camera's, light the light's (views set with set_view); returns the image [H, W, 4]."""
+        assert self.kind == "ref"
+        out = np.zeros((self.H, self.W, 4), np.float32)
+        assert self.lib.ref_reconstruct_dof_motion_shadows(self.h, light.h, f32p(out)) == 0
+        return out
 
     def shadows(self, queries, density):
         """TreeGather::reconstructShadows of the reference build: queries [H, W, qspp, 16],
