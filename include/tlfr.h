@@ -242,7 +242,7 @@ typedef struct tlfr_view
  * sqrt(camera_density) of the nearest sample (the camera buffer's
  * LIGHTSPACE_DENSITY channel, one float per input record in record order;
  * NULL reads 1); the colour is lit by 1.5 * max(0, -L.N) with N rebuilt from
- * the nearest sample's w gradients (lightSpaceDot, Util.cpp:201-224), plus
+ * the nearest sample's w gradients (lightSpaceDot, Util.cpp:202-224), plus
  * 0.5 * ambient * the camera colour.  Samples beyond camera far - 0.01 or
  * outside the light's image keep the camera colour; a pixel with an output
  * sample the camera cannot reconstruct is red.  rgba: W*H*4 floats (device

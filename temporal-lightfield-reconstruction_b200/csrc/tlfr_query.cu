@@ -2309,7 +2309,7 @@ k_query_shadow_large(QParams P, const float* __restrict__ queries, const int* __
 // (Sobol dimensions 3 and 4 of the sample, rotated per pixel) moves it across
 // the light's lens; the light's hierarchy reconstructs it in shadow mode, and
 // the result is shaded with the normal rebuilt from the nearest sample's w
-// gradients (lightSpaceDot, viewSpaceNormalFromWGradients, Util.cpp:170-224).
+// gradients (lightSpaceDot, viewSpaceNormalFromWGradients, Util.cpp:174-224).
 // The matrix and vector arithmetic keeps the framework's operation order
 // (framework/base/Math.hpp: sums accumulate from 0 in index order, rcp(0) = 0,
 // normalized = v * (1 * rcp(length))), so the results are bit-identical.
