@@ -613,8 +613,13 @@ constexpr int kBlock = 128;
 // capacities of the full per-query path (statistics pass and heavy pass)
 constexpr int kStackCap = 96, kLeafCap = 256, kRsCap = 512, kSurfCap = 64;
 // capacities of the light pass: traversal stack and leaf list per output
-// sample, both in shared memory
+// sample, both in shared memory.  kLLeaf is also the most leaves the warp's
+// scan holds (one per lane).  The single-frame path runs a first light pass
+// with fewer leaves (kL1Leaf), which fits six blocks per SM, and retries the
+// output samples that outgrow it with the full kLLeaf and a deeper stack.
 constexpr int kLStack = 16, kLLeaf = 32;
+constexpr int kL1Stack = 16, kL1Leaf = 28;
+constexpr int kL2Stack = 32, kL2Leaf = 32;
 
 // Per-thread column of a shared-memory array laid out [slot][thread]: a warp
 // whose lanes touch different slots still hits distinct banks.  The host build
@@ -742,9 +747,11 @@ TLFR_HD int collect_pairs(const QParams& P, const Column<int>& stack, int stack_
 }
 
 // Light pass, part 1: each lane collects its own output sample's leaves at 1R.
+template <int LEAF, int STACK>
 TLFR_HD int light_collect(const QParams& P, const Column<int>& stack, const Column<float2>& leaves, const Query& o)
 {
-    return collect_pairs(P, stack, kLStack, leaves, kLLeaf, o, P.disp0);
+    static_assert(LEAF <= 32, "the warp's scan holds one leaf per lane");
+    return collect_pairs(P, stack, STACK, leaves, LEAF, o, P.disp0);
 }
 
 // sameSurface's sixteen plane values of one node for one output sample: each
@@ -1025,8 +1032,16 @@ constexpr int kQueueRestart = 1 << 30;
 
 constexpr int kProbe = 4;
 // resident light-pass blocks per SM: shared memory (40 KB per block) allows 5,
-// and a 5-block register budget (<= 102 per thread) measured 9% faster than 4
+// and a 5-block register budget (<= 102 per thread) measured 9% faster than 4.
+// The first pass of the single-frame path (36 KB) fits 6; its retry pass
+// (48 KB) 4.
 constexpr int kLightBlocksPerSM = 5;
+constexpr int kL1BlocksPerSM = 6;
+constexpr int kL2BlocksPerSM = 4;
+// Light-pass kinds: every output sample of a map, overflow to the full path
+// (kLightPlain); the same with overflow to a retry list (kLightFirst); the
+// output samples of a retry list (kLightRetry), overflow to the full path.
+enum { kLightPlain = 0, kLightFirst = 1, kLightRetry = 2 };
 
 // PROBE: the router's coarse pass.  Query k of pixel p is output sample
 // (k % kProbe) * M / kProbe (four per pixel); nothing is written but the count of
@@ -1083,26 +1098,38 @@ __device__ __forceinline__ bool light_query_id(const QParams& P, const LightMap&
 }
 
 // Shared-memory columns of a light-pass block.
+template <int LEAF, int STACK>
 struct LightShared
 {
-    float2 leaves[kLLeaf][kBlock];
-    int stack[kLStack][kBlock];
+    float2 leaves[LEAF][kBlock];
+    int stack[STACK][kBlock];
 };
 
-// One block iteration u of the light pass.
-template <bool PROBE>
+// One block iteration u of the light pass.  kLightRetry: the output samples
+// are retry[u * kBlock + thread] for indices below num_queries; kLightFirst:
+// those that outgrow the capacities are appended to retry.
+template <bool PROBE, int LEAF, int STACK, int MODE>
 __device__ __forceinline__ void light_unit(const QParams& P, const LightMap& L, long long u, long long num_queries,
                                            float4* __restrict__ qcol, int* __restrict__ heavy,
-                                           int* __restrict__ heavy_count, LightShared& sh)
+                                           int* __restrict__ heavy_count, LightShared<LEAF, STACK>& sh,
+                                           int* __restrict__ retry = nullptr, int* __restrict__ retry_count = nullptr)
 {
-    float2 (&sh_leaves)[kLLeaf][kBlock] = sh.leaves;
+    float2 (&sh_leaves)[LEAF][kBlock] = sh.leaves;
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
     const Column<int> stack{ &sh.stack[0][threadIdx.x], kBlock };
     {
         // each lane: traversal and leaf sort of its own output sample
         long long q = 0;
-        const bool valid = light_query_id(P, L, u, threadIdx.x, num_queries, q);
+        bool valid;
+        if (MODE == kLightRetry)
+        {
+            const long long k = u * kBlock + threadIdx.x;
+            valid = k < num_queries;
+            q = valid ? retry[k] : 0;
+        }
+        else
+            valid = light_query_id(P, L, u, threadIdx.x, num_queries, q);
         Query o{};
         int nl = -2;
         const long long pix = valid ? (PROBE ? q / kProbe : q / P.M) : 0;
@@ -1111,7 +1138,7 @@ __device__ __forceinline__ void light_unit(const QParams& P, const LightMap& L, 
         {
             o = PROBE ? make_query(P, (int)(pix % P.W), (int)(pix / P.W), (int)((q % kProbe) * P.M / kProbe))
                       : query_of(P, q);
-            nl = light_collect(P, stack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, o);
+            nl = light_collect<LEAF, STACK>(P, stack, Column<float2>{ &sh_leaves[0][threadIdx.x], kBlock }, o);
         }
         const unsigned fast_lanes = __ballot_sync(0xffffffffu, fast);
         __syncwarp();
@@ -1146,12 +1173,14 @@ __device__ __forceinline__ void light_unit(const QParams& P, const LightMap& L, 
                 atomicAdd(&heavy_count[pix], 1);
             return;
         }
-        bool hv = false;
+        bool hv = false, rt = false;
         int entry = 0;
         if (valid)
         {
             if (code == 0)
                 qcol[q] = col;
+            else if (MODE == kLightFirst && code == 2)
+                rt = true;
             else
             {
                 hv = true;
@@ -1159,18 +1188,35 @@ __device__ __forceinline__ void light_unit(const QParams& P, const LightMap& L, 
             }
         }
         warp_append(heavy, heavy_count, hv, entry);
+        if (MODE == kLightFirst)
+            warp_append(retry, retry_count, rt, (int)q);
     }
 }
 
-template <bool PROBE>
-__global__ void __launch_bounds__(kBlock, kLightBlocksPerSM)
+// The light pass over a map (kLightPlain, kLightFirst) or over a retry list
+// of *retry_count output samples (kLightRetry).
+template <bool PROBE, int LEAF, int STACK, int BLOCKS_PER_SM, int MODE>
+__global__ void __launch_bounds__(kBlock, BLOCKS_PER_SM)
 k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__ qcol, int* __restrict__ heavy,
-              int* __restrict__ heavy_count)
+              int* __restrict__ heavy_count, int* __restrict__ retry, int* __restrict__ retry_count)
 {
-    __shared__ LightShared sh;
-    for (long long u = blockIdx.x; u < L.units; u += gridDim.x)
-        light_unit<PROBE>(P, L, u, num_queries, qcol, heavy, heavy_count, sh);
+    __shared__ LightShared<LEAF, STACK> sh;
+    if (MODE == kLightRetry)
+    {
+        const long long n = *retry_count;
+        for (long long u = blockIdx.x; u * kBlock < n; u += gridDim.x)
+            light_unit<PROBE, LEAF, STACK, MODE>(P, L, u, n, qcol, heavy, heavy_count, sh, retry);
+    }
+    else
+        for (long long u = blockIdx.x; u < L.units; u += gridDim.x)
+            light_unit<PROBE, LEAF, STACK, MODE>(P, L, u, num_queries, qcol, heavy, heavy_count, sh, retry,
+                                                 retry_count);
 }
+
+// the light-pass instances
+#define K_LIGHT_PLAIN(PROBE) k_query_light<PROBE, kLLeaf, kLStack, kLightBlocksPerSM, kLightPlain>
+#define K_LIGHT_FIRST k_query_light<false, kL1Leaf, kL1Stack, kL1BlocksPerSM, kLightFirst>
+#define K_LIGHT_RETRY k_query_light<false, kL2Leaf, kL2Stack, kL2BlocksPerSM, kLightRetry>
 
 // ---------------------------------------------------------------------------
 // Pass 2, warp-cooperative: output samples known to need the 2R fetch (the
@@ -2693,7 +2739,7 @@ tlfr_status route_probe(Ctx& c, int* d_counts)
     CKQ(cudaMemsetAsync(d_counts, 0, sizeof(int) * npix, s));
     const LightMap L = light_map(c, nq);
     const int blocks = (int)std::min<long long>(L.units, (long long)c.num_sms * 64);
-    TLFR_LAUNCH(c, k_query_light<true>, blocks, kBlock, s, P, L, nq, nullptr, nullptr, d_counts);
+    TLFR_LAUNCH(c, K_LIGHT_PLAIN(true), blocks, kBlock, s, P, L, nq, nullptr, nullptr, d_counts, nullptr, nullptr);
     CKQ(cudaGetLastError());
     return TLFR_OK;
 }
@@ -2752,7 +2798,7 @@ __global__ void __launch_bounds__(kBlock, kLightBlocksPerSM)
 k_batch_light(const FrameDesc* __restrict__ fd, const long long* __restrict__ unit_begin, int nframes,
               unsigned long long* __restrict__ next_unit)
 {
-    __shared__ LightShared sh;
+    __shared__ LightShared<kLLeaf, kLStack> sh;
     __shared__ QParams sP;
     __shared__ LightMap sL;
     __shared__ long long sU;
@@ -2779,7 +2825,8 @@ k_batch_light(const FrameDesc* __restrict__ fd, const long long* __restrict__ un
             break;
         cur = f;
         const FrameDesc& D = fd[f];
-        light_unit<false>(sP, sL, u - unit_begin[f], D.nq, D.qcol, D.heavy, D.counters + 2, sh);
+        light_unit<false, kLLeaf, kLStack, kLightPlain>(sP, sL, u - unit_begin[f], D.nq, D.qcol, D.heavy,
+                                                         D.counters + 2, sh);
         __syncthreads();
     }
 }
@@ -2911,7 +2958,7 @@ static tlfr_status light_trial(const FrameDesc& D, const Ctx& c, int shape, cuda
     const int blocks = (int)std::min<long long>(L.units, (long long)c.num_sms * 64);
     CKB(cudaMemsetAsync(D.counters, 0, 4 * sizeof(int), s));
     CKB(cudaEventRecord(e0, s));
-    k_query_light<false><<<blocks, kBlock, 0, s>>>(D.P, L, D.nq, D.qcol, D.heavy, D.counters + 2);
+    K_LIGHT_PLAIN(false)<<<blocks, kBlock, 0, s>>>(D.P, L, D.nq, D.qcol, D.heavy, D.counters + 2, nullptr, nullptr);
     CKB(cudaEventRecord(e1, s));
     CKB(cudaEventSynchronize(e1));
     CKB(cudaEventElapsedTime(ms, e0, e1));
@@ -3290,7 +3337,7 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
         return fb;
     if (c.params.enable_cuda)
         return reconstruct_toggle(c, d_rgba);
-    int* counters = reinterpret_cast<int*>(c.d_stats + 1);   // [0] overflow, [1] hard, [2] heavy
+    int* counters = reinterpret_cast<int*>(c.d_stats + 1);   // [0] overflow, [1] hard, [2] heavy, [3] retry
     QParams P = make_params(c);
     CKQ(cudaMemsetAsync(c.d_stats, 0, sizeof(DevStats) + 8 * sizeof(int), s));
     if ((c.router || c.route_all_fast) && !c.route_prob)
@@ -3343,8 +3390,13 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
             c.coop_scratch_bytes = coop_scratch_bytes(c.num_sms);
             CKQ(cudaMalloc(&c.coop_scratch, c.coop_scratch_bytes));
         }
-        TLFR_LAUNCH(c, k_query_light<false>, light_default_blocks(c), kBlock, s, P, light_map(c), nq, c.qcol,
-                    c.heavy_queue, counters + 2);
+        // first light pass; the output samples that outgrow it are retried with
+        // larger capacities (the retry list lives in the overflow queue, which
+        // the full-path pass only fills after the retry pass has read it)
+        TLFR_LAUNCH(c, K_LIGHT_FIRST, light_default_blocks(c), kBlock, s, P, light_map(c), nq, c.qcol,
+                    c.heavy_queue, counters + 2, c.ovf_queue, counters + 3);
+        TLFR_LAUNCH(c, K_LIGHT_RETRY, c.num_sms * kL2BlocksPerSM, kBlock, s, P, light_map(c), nq, c.qcol,
+                    c.heavy_queue, counters + 2, c.ovf_queue, counters + 3);
         CKQ(cudaEventRecord(c.evq1, s));
         TLFR_LAUNCH(c, k_query_coop, coop_blocks(c), kCWarps * 32, s, P, c.heavy_queue, counters + 2, c.qcol,
                     c.ovf_queue, counters + 0, (int)c.ovf_cap, reinterpret_cast<CoopScratch*>(c.coop_scratch));
