@@ -615,11 +615,11 @@ constexpr int kStackCap = 96, kLeafCap = 256, kRsCap = 512, kSurfCap = 64;
 // capacities of the light pass: traversal stack and leaf list per output
 // sample, both in shared memory.  kLLeaf is also the most leaves the warp's
 // scan holds (one per lane).  The single-frame path runs a first light pass
-// with fewer leaves (kL1Leaf), which fits six blocks per SM, and retries the
+// with fewer leaves (kL1Leaf), which fits seven blocks per SM, and retries the
 // output samples that outgrow it with the full kLLeaf and a deeper stack.
 constexpr int kLStack = 16, kLLeaf = 32;
-constexpr int kL1Stack = 16, kL1Leaf = 28;
-constexpr int kL2Stack = 32, kL2Leaf = 32;
+constexpr int kL1Stack = 12, kL1Leaf = 24;
+constexpr int kL2Stack = 30, kL2Leaf = 32;
 
 // Per-thread column of a shared-memory array laid out [slot][thread]: a warp
 // whose lanes touch different slots still hits distinct banks.  The host build
@@ -1033,10 +1033,11 @@ constexpr int kQueueRestart = 1 << 30;
 constexpr int kProbe = 4;
 // resident light-pass blocks per SM: shared memory (40 KB per block) allows 5,
 // and a 5-block register budget (<= 102 per thread) measured 9% faster than 4.
-// The first pass of the single-frame path (36 KB) fits 6; its retry pass
-// (48 KB) 4.
+// The first tier (24 leaves, 12 stack entries: 30 KB) fits 7 at <= 72
+// registers (a few spilled): 1340 ms per 1920x1080x8 frame against 1378 at
+// 6 blocks with 28 leaves and 1492 with one tier; the retry tier (47 KB) 4.
 constexpr int kLightBlocksPerSM = 5;
-constexpr int kL1BlocksPerSM = 6;
+constexpr int kL1BlocksPerSM = 7;
 constexpr int kL2BlocksPerSM = 4;
 // Light-pass kinds: every output sample of a map, overflow to the full path
 // (kLightPlain); the same with overflow to a retry list (kLightFirst); the
@@ -2771,7 +2772,7 @@ struct FrameDesc
     float4* qcol;
     int* heavy;
     int* ovf;
-    int* counters;          // [0] overflow queue, [1] capacity failures, [2] heavy queue
+    int* counters;          // [0] overflow queue, [1] capacity failures, [2] heavy queue, [3] retry list
     float4* out;
 };
 
@@ -2794,11 +2795,16 @@ __device__ __forceinline__ int frame_of(const long long* __restrict__ begin, int
 }
 
 // Light pass over every frame of a chunk: a block takes one unit at a time.
-__global__ void __launch_bounds__(kBlock, kLightBlocksPerSM)
+// FIRST: every output sample of every frame (LightMap units), those that
+// outgrow the first tier's capacities appended to the frame's retry list (its
+// overflow queue, counters[3]); otherwise the retry lists (units of kBlock
+// entries, offsets from k_batch_retry_units), overflow to the full path.
+template <bool FIRST>
+__global__ void __launch_bounds__(kBlock, FIRST ? kL1BlocksPerSM : kL2BlocksPerSM)
 k_batch_light(const FrameDesc* __restrict__ fd, const long long* __restrict__ unit_begin, int nframes,
               unsigned long long* __restrict__ next_unit)
 {
-    __shared__ LightShared<kLLeaf, kLStack> sh;
+    __shared__ LightShared<FIRST ? kL1Leaf : kL2Leaf, FIRST ? kL1Stack : kL2Stack> sh;
     __shared__ QParams sP;
     __shared__ LightMap sL;
     __shared__ long long sU;
@@ -2825,10 +2831,28 @@ k_batch_light(const FrameDesc* __restrict__ fd, const long long* __restrict__ un
             break;
         cur = f;
         const FrameDesc& D = fd[f];
-        light_unit<false, kLLeaf, kLStack, kLightPlain>(sP, sL, u - unit_begin[f], D.nq, D.qcol, D.heavy,
-                                                         D.counters + 2, sh);
+        if constexpr (FIRST)
+            light_unit<false, kL1Leaf, kL1Stack, kLightFirst>(sP, sL, u - unit_begin[f], D.nq, D.qcol, D.heavy,
+                                                              D.counters + 2, sh, D.ovf, D.counters + 3);
+        else
+            light_unit<false, kL2Leaf, kL2Stack, kLightRetry>(sP, sL, u - unit_begin[f], D.counters[3], D.qcol,
+                                                              D.heavy, D.counters + 2, sh, D.ovf);
         __syncthreads();
     }
+}
+
+// Units of the retry pass: kBlock retried output samples each.
+__global__ void k_batch_retry_units(const FrameDesc* __restrict__ fd, int nframes, long long* __restrict__ unit_begin)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    long long acc = 0;
+    for (int f = 0; f < nframes; f++)
+    {
+        unit_begin[f] = acc;
+        acc += (fd[f].counters[3] + kBlock - 1) / kBlock;
+    }
+    unit_begin[nframes] = acc;
 }
 
 // Work items of the full-path pass: 32 queued output samples each.
@@ -2902,7 +2926,8 @@ struct BatchChunk
     long long* d_unit_begin = nullptr;  // count + 1
     long long* d_item_begin = nullptr;  // count + 1
     long long* d_pix_begin = nullptr;   // count + 1
-    unsigned long long* d_work = nullptr;   // [0] next light unit, [1] next full-path item
+    long long* d_retry_begin = nullptr; // count + 1
+    unsigned long long* d_work = nullptr;   // [0] next light unit, [1] next full-path item, [2] next retry unit
 };
 
 struct BatchPlan
@@ -3113,15 +3138,15 @@ tlfr_status batch_build(BatchPlan& bp, const std::vector<BatchEntry>& entries, c
     }
     // device tables
     CKB(cudaMalloc(&bp.d_desc, sizeof(FrameDesc) * n));
-    CKB(cudaMalloc(&bp.d_offsets, sizeof(long long) * 3 * (n + bp.chunks.size())));
-    CKB(cudaMalloc(&bp.d_work, sizeof(unsigned long long) * 2 * bp.chunks.size()));
+    CKB(cudaMalloc(&bp.d_offsets, sizeof(long long) * 4 * (n + bp.chunks.size())));
+    CKB(cudaMalloc(&bp.d_work, sizeof(unsigned long long) * 3 * bp.chunks.size()));
     std::vector<long long> offs;
-    offs.reserve(3 * (n + bp.chunks.size()));
+    offs.reserve(4 * (n + bp.chunks.size()));
     for (size_t k = 0; k < bp.chunks.size(); k++)
     {
         BatchChunk& ch = bp.chunks[k];
         ch.d_desc = bp.d_desc + ch.first;
-        ch.d_work = bp.d_work + 2 * k;
+        ch.d_work = bp.d_work + 3 * k;
         const size_t base = offs.size();
         long long u = 0, pxl = 0;
         std::vector<long long> ub, pb;
@@ -3136,10 +3161,11 @@ tlfr_status batch_build(BatchPlan& bp, const std::vector<BatchEntry>& entries, c
         pb.push_back(pxl);
         offs.insert(offs.end(), ub.begin(), ub.end());
         offs.insert(offs.end(), pb.begin(), pb.end());
-        offs.insert(offs.end(), ch.count + 1, 0LL);      // item offsets, filled on the device
+        offs.insert(offs.end(), 2 * (ch.count + 1), 0LL);    // item and retry offsets, filled on the device
         ch.d_unit_begin = bp.d_offsets + base;
         ch.d_pix_begin = bp.d_offsets + base + ch.count + 1;
         ch.d_item_begin = bp.d_offsets + base + 2 * (ch.count + 1);
+        ch.d_retry_begin = bp.d_offsets + base + 3 * (ch.count + 1);
     }
     CKB(cudaMemcpy(bp.d_offsets, offs.data(), sizeof(long long) * offs.size(), cudaMemcpyHostToDevice));
     CKB(cudaMemcpy(bp.d_desc, bp.desc.data(), sizeof(FrameDesc) * n, cudaMemcpyHostToDevice));
@@ -3153,7 +3179,7 @@ tlfr_status batch_enqueue(BatchPlan& bp, cudaStream_t s, std::string& err, long 
     const int n = (int)bp.entries.size();
     long long L = 0;
     CKB(cudaMemsetAsync(bp.d_counters, 0, sizeof(int) * 4 * n, s));
-    CKB(cudaMemsetAsync(bp.d_work, 0, sizeof(unsigned long long) * 2 * bp.chunks.size(), s));
+    CKB(cudaMemsetAsync(bp.d_work, 0, sizeof(unsigned long long) * 3 * bp.chunks.size(), s));
     for (const BatchChunk& ch : bp.chunks)
     {
         // the router's flags for this chunk's routed frames (their descriptors
@@ -3176,13 +3202,18 @@ tlfr_status batch_enqueue(BatchPlan& bp, cudaStream_t s, std::string& err, long 
                 return rs;
             L += 7;
         }
-        const int lb = bp.num_sms * kLightBlocksPerSM;
-        k_batch_light<<<lb, kBlock, 0, s>>>(ch.d_desc, ch.d_unit_begin, ch.count, ch.d_work + 0);
+        // first light pass, then the retry lists (in the frames' overflow
+        // queues, which the full-path pass fills only after they are read)
+        k_batch_light<true><<<bp.num_sms * kL1BlocksPerSM, kBlock, 0, s>>>(ch.d_desc, ch.d_unit_begin, ch.count,
+                                                                         ch.d_work + 0);
+        k_batch_retry_units<<<1, 32, 0, s>>>(ch.d_desc, ch.count, ch.d_retry_begin);
+        k_batch_light<false><<<bp.num_sms * kL2BlocksPerSM, kBlock, 0, s>>>(ch.d_desc, ch.d_retry_begin, ch.count,
+                                                                          ch.d_work + 2);
         k_batch_items<<<1, 32, 0, s>>>(ch.d_desc, ch.count, ch.d_item_begin);
         k_batch_coop<<<bp.num_sms * kCoopBlocksPerSM, kCWarps * 32, 0, s>>>(ch.d_desc, ch.d_item_begin, ch.count,
                                                                            ch.d_work + 1,
                                                                            reinterpret_cast<CoopScratch*>(bp.coop_scratch));
-        L += 3;
+        L += 5;
         for (int f = ch.first; f < ch.first + ch.count; f++)
         {
             const FrameDesc& D = bp.desc[f];
