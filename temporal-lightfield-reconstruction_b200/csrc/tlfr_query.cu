@@ -1334,8 +1334,20 @@ __device__ int traverse_sorted(const QParams& P, const Query& o, float R, Leaf* 
 // quadrant mask and first strict minimum.  All lanes call it with the same
 // arguments; returns the accepted count (same on all lanes) or -1 when rs /
 // surf outgrow the scratch.
+constexpr int kTriMax = 200;                    // n >= 200 is accepted without the search (RO.cpp:215)
+constexpr int kTriWords = (kTriMax + 31) / 32;
+
+// Per-warp shared memory of the full path: the coverage search's bit rows, and
+// the sameSurface values of the current group of 32 leaves ([value][leaf]).
+struct CoopShared
+{
+    unsigned row[kTriWords];                    // samples l > m within 2*dispersion of m
+    unsigned mask[5 * kTriWords];               // quadrant patterns 3, 6, 9, 12; within dispersion
+    float sv[16][32];
+};
+
 __device__ int coop_scan(const QParams& P, const Query& o, float R, const Leaf* leaves, int nleaves,
-                         CoopScratch& S, int& nsurf_out)
+                         CoopScratch& S, CoopShared& T, int& nsurf_out)
 {
     const int lane = threadIdx.x & 31;
     const float RANGE = 1.0f / sqrtf(128.0f);
@@ -1350,12 +1362,22 @@ __device__ int coop_scan(const QParams& P, const Query& o, float R, const Leaf* 
     {
         const int ng = mini(32, nleaves - g);
         int my_s0 = 0, my_n = 0;
+        __syncwarp();   // the previous group's values have been read
         if (lane < ng)
         {
-            const int4 d = P.nodes[leaves[g + lane].node].d;
-            my_s0 = d.z;
-            my_n = d.w - d.z;
+            const QNode nd = load_node(P.nodes, leaves[g + lane].node);
+            my_s0 = nd.d.z;
+            my_n = nd.d.w - nd.d.z;
+            SurfVals v;
+            surf_vals(nd, uvtmin, uvtmax, v);
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+            {
+                T.sv[2 * a][lane] = v.v[a][0];
+                T.sv[2 * a + 1][lane] = v.v[a][1];
+            }
         }
+        __syncwarp();
         int my_f = my_n;
         for (int off = 1; off < 32; off <<= 1)
         {
@@ -1400,11 +1422,35 @@ __device__ int coop_scan(const QParams& P, const Query& o, float R, const Leaf* 
                     bool same = true;
                     if (nsurf > 0)
                     {
-                        const QNode node = load_node(P.nodes, leaves[lidx].node);
-                        for (int jb = surfaceStart; jb < lidx && same; jb += 32)
+                        // leaves of earlier groups since the surface opened (rare)
+                        if (surfaceStart < g)
                         {
-                            const int j = jb + lane;
-                            const bool ok = (j < lidx) ? same_surface(node, load_node(P.nodes, leaves[j].node), uvtmin, uvtmax) : true;
+                            const QNode node = load_node(P.nodes, leaves[lidx].node);
+                            for (int jb = surfaceStart; jb < g && same; jb += 32)
+                            {
+                                const int j = jb + lane;
+                                const bool ok = (j < g) ? same_surface(node, load_node(P.nodes, leaves[j].node), uvtmin, uvtmax) : true;
+                                same = __all_sync(0xffffffffu, ok);
+                            }
+                        }
+                        // this group's leaves: lane j - g tests leaf j from the precomputed values
+                        if (same)
+                        {
+                            const int j = g + lane;
+                            bool ok = true;
+                            if (j >= surfaceStart && j < lidx)
+                            {
+                                SurfVals cur, mine;
+#pragma unroll
+                                for (int a = 0; a < 8; a++)
+                                {
+                                    cur.v[a][0] = T.sv[2 * a][kseg];
+                                    cur.v[a][1] = T.sv[2 * a + 1][kseg];
+                                    mine.v[a][0] = T.sv[2 * a][lane];
+                                    mine.v[a][1] = T.sv[2 * a + 1][lane];
+                                }
+                                ok = same_surface_vals(cur, mine);
+                            }
                             same = __all_sync(0xffffffffu, ok);
                         }
                     }
@@ -1483,16 +1529,9 @@ __device__ __forceinline__ void coop_reverse(RSample* a, int lo, int hi)     // 
 // beyond k that complete the quadrants (bit masks per quadrant pattern) and the
 // within-dispersion condition (a bit mask), each checked against k's side
 // length before the edge functions.
-constexpr int kTriMax = 200;                    // n >= 200 is accepted without the search (RO.cpp:215)
-constexpr int kTriWords = (kTriMax + 31) / 32;
 
-struct TriShared
-{
-    unsigned row[kTriWords];                    // samples l > m within 2*dispersion of m
-    unsigned mask[5 * kTriWords];               // quadrant patterns 3, 6, 9, 12; within dispersion
-};
 
-__device__ bool coop_triangle(const RSample* in, int n, const Query& o, float dispersion, TriShared& T)
+__device__ bool coop_triangle(const RSample* in, int n, const Query& o, float dispersion, CoopShared& T)
 {
     const int lane = threadIdx.x & 31;
     const int W = (n + 31) >> 5;
@@ -1589,7 +1628,7 @@ __device__ bool coop_triangle(const RSample* in, int n, const Query& o, float di
 // path, with the warp's working lists S and shared triangle-search bits T.
 __device__ __forceinline__ void coop_group(const QParams& P, const int* __restrict__ queue, int n, int b,
                                            float4* __restrict__ qcol, int* __restrict__ ovf_queue,
-                                           int* __restrict__ ovf_count, int ovf_cap, CoopScratch& S, TriShared& T)
+                                           int* __restrict__ ovf_count, int ovf_cap, CoopScratch& S, CoopShared& T)
 {
     const int lane = threadIdx.x & 31;
     {
@@ -1637,7 +1676,7 @@ __device__ __forceinline__ void coop_group(const QParams& P, const int* __restri
             if (!ovf && __shfl_sync(0xffffffffu, restart, j))
             {
                 // the 1R fetch and the fetch2R decision (RO.cpp:94-99)
-                total = coop_scan(P, o, dispersion, S.leaves[j], nl, S, nsurf);
+                total = coop_scan(P, o, dispersion, S.leaves[j], nl, S, T, nsurf);
                 ovf = total < 0;
                 if (!ovf)
                     fetch2R = nsurf == 0 || (S.surf[0].quad != 0xF && nsurf > 1);
@@ -1649,7 +1688,7 @@ __device__ __forceinline__ void coop_group(const QParams& P, const int* __restri
             }
             if (!ovf && fetch2R)
             {
-                total = coop_scan(P, o, dispersion * 2, S.leaves[j], nl, S, nsurf);
+                total = coop_scan(P, o, dispersion * 2, S.leaves[j], nl, S, T, nsurf);
                 ovf = total < 0;
             }
             // widening when 2R found nothing (RO.cpp:110-120); lane 0 traverses
@@ -1662,7 +1701,7 @@ __device__ __forceinline__ void coop_group(const QParams& P, const int* __restri
                 cnt = __shfl_sync(0xffffffffu, cnt, 0);
                 __syncwarp();
                 if (cnt < 0) { ovf = true; break; }
-                total = coop_scan(P, o, dispersion * 2, S.leaves[j], cnt, S, nsurf);
+                total = coop_scan(P, o, dispersion * 2, S.leaves[j], cnt, S, T, nsurf);
                 ovf = total < 0;
             }
             if (ovf)
@@ -1797,7 +1836,7 @@ k_query_coop(QParams P, const int* __restrict__ queue, const int* __restrict__ q
              float4* __restrict__ qcol, int* __restrict__ ovf_queue, int* __restrict__ ovf_count, int ovf_cap,
              CoopScratch* __restrict__ scratch)
 {
-    __shared__ TriShared sh_tri[kCWarps];
+    __shared__ CoopShared sh_tri[kCWarps];
     const int warp = blockIdx.x * kCWarps + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * kCWarps;
     const int n = *queue_count;
@@ -2874,7 +2913,7 @@ __global__ void __launch_bounds__(kCWarps * 32, TLFR_COOP_BLOCKS_PER_SM)
 k_batch_coop(const FrameDesc* __restrict__ fd, const long long* __restrict__ item_begin, int nframes,
              unsigned long long* __restrict__ next_item, CoopScratch* __restrict__ scratch)
 {
-    __shared__ TriShared sh_tri[kCWarps];
+    __shared__ CoopShared sh_tri[kCWarps];
     const int lane = threadIdx.x & 31;
     const int warp = blockIdx.x * kCWarps + (threadIdx.x >> 5);
     const long long total = item_begin[nframes];
