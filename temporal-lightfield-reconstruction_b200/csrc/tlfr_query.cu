@@ -1673,36 +1673,41 @@ __device__ __forceinline__ void coop_group(const QParams& P, const int* __restri
             float dispersion = P.disp0;
             int nsurf = 0, total = 0;
             bool fetch2R = true;
-            if (!ovf && __shfl_sync(0xffffffffu, restart, j))
+            // The fetches, through one call site of the scan (the kernel's
+            // instruction footprint is what limits it): step 0 the 1R fetch of a
+            // restarted sample and its fetch2R decision (RO.cpp:94-99), step 1
+            // the 2R fetch, steps 2-4 the widening while nothing was found
+            // (RO.cpp:110-120; lane 0 traverses).
+            bool set_aside = false;
+            for (int step = __shfl_sync(0xffffffffu, restart, j) ? 0 : 1; !ovf && step <= 4; step++)
             {
-                // the 1R fetch and the fetch2R decision (RO.cpp:94-99)
-                total = coop_scan(P, o, dispersion, S.leaves[j], nl, S, T, nsurf);
-                ovf = total < 0;
-                if (!ovf)
-                    fetch2R = nsurf == 0 || (S.surf[0].quad != 0xF && nsurf > 1);
-                if (!ovf && fetch2R)
+                if (step >= 2)
                 {
-                    redo |= 1u << j;     // the 2R fetch in the second round
-                    continue;
+                    dispersion *= 2.f;
+                    int cnt = 0;
+                    if (lane == 0)
+                        cnt = traverse_sorted(P, o, dispersion * 2, S.leaves[j], kCLeaf);
+                    nl = __shfl_sync(0xffffffffu, cnt, 0);
+                    __syncwarp();
+                    if (nl < 0) { ovf = true; break; }
                 }
-            }
-            if (!ovf && fetch2R)
-            {
-                total = coop_scan(P, o, dispersion * 2, S.leaves[j], nl, S, T, nsurf);
+                total = coop_scan(P, o, step == 0 ? dispersion : dispersion * 2, S.leaves[j], nl, S, T, nsurf);
                 ovf = total < 0;
+                if (ovf)
+                    break;
+                if (step == 0)
+                {
+                    fetch2R = nsurf == 0 || (S.surf[0].quad != 0xF && nsurf > 1);
+                    set_aside = fetch2R;     // the 2R fetch in the second round
+                    break;
+                }
+                if (total != 0)
+                    break;
             }
-            // widening when 2R found nothing (RO.cpp:110-120); lane 0 traverses
-            for (int k = 0; k < 3 && !ovf && fetch2R && total == 0; k++)
+            if (set_aside)
             {
-                dispersion *= 2.f;
-                int cnt = 0;
-                if (lane == 0)
-                    cnt = traverse_sorted(P, o, dispersion * 2, S.leaves[j], kCLeaf);
-                cnt = __shfl_sync(0xffffffffu, cnt, 0);
-                __syncwarp();
-                if (cnt < 0) { ovf = true; break; }
-                total = coop_scan(P, o, dispersion * 2, S.leaves[j], cnt, S, T, nsurf);
-                ovf = total < 0;
+                redo |= 1u << j;
+                continue;
             }
             if (ovf)
             {
