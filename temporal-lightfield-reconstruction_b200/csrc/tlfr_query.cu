@@ -1640,23 +1640,21 @@ __device__ __forceinline__ void coop_group(const QParams& P, const int* __restri
         const bool valid = entry >= 0;
         const int myq = valid ? (entry & ~kQueueRestart) : 0;
         Query myo = query_of(P, myq);
-        int mycount = valid ? traverse_sorted(P, myo, restart ? P.disp0 : P.disp0 * 2, S.leaves[lane], kCLeaf) : 0;
-        __syncwarp();
+        int mycount = 0;
         // 2. each sample of the batch by the whole warp.  A restarted sample whose
         // 1R fetch ends with fetch2R true is set aside; its lane traverses at 2R
-        // (all such lanes in parallel) and it runs again in a second round.
+        // (all such lanes in parallel) and it runs again in a second round.  Both
+        // rounds' traversals share one call site.
         unsigned todo = __ballot_sync(0xffffffffu, valid);
         for (int round = 0; round < 2 && todo; round++)
         {
-        if (round == 1)
+        if ((todo >> lane) & 1u)
         {
-            if ((todo >> lane) & 1u)
-            {
-                mycount = traverse_sorted(P, myo, P.disp0 * 2, S.leaves[lane], kCLeaf);
+            if (round == 1)
                 restart = false;
-            }
-            __syncwarp();
+            mycount = traverse_sorted(P, myo, restart ? P.disp0 : P.disp0 * 2, S.leaves[lane], kCLeaf);
         }
+        __syncwarp();
         unsigned redo = 0;
         for (unsigned jm = todo; jm; jm &= jm - 1)
         {
