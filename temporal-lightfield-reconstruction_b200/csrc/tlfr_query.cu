@@ -1641,26 +1641,27 @@ __device__ __forceinline__ void coop_group(const QParams& P, const int* __restri
         const int myq = valid ? (entry & ~kQueueRestart) : 0;
         Query myo = query_of(P, myq);
         int mycount = 0;
-        // 2. each sample of the batch by the whole warp.  A restarted sample whose
-        // 1R fetch ends with fetch2R true is set aside; its lane traverses at 2R
-        // (all such lanes in parallel) and it runs again in a second round.  Both
-        // rounds' traversals share one call site.
+        float mydisp = P.disp0;     // this lane's dispersion (doubled by each widening)
+        int mywiden = 0;
+        // 2. each sample of the batch by the whole warp, in rounds.  A sample is
+        // set aside for the next round (its lane traverses again, all such lanes
+        // in parallel) when a restarted sample's 1R fetch ends with fetch2R true
+        // (RO.cpp:94-99; the next round fetches at 2R), and when a 2R fetch found
+        // nothing (the widening, RO.cpp:110-120: at most three times, each
+        // doubling the dispersion).  Every traversal and every fetch goes through
+        // one call site (the kernel's instruction footprint is what limits it).
         unsigned todo = __ballot_sync(0xffffffffu, valid);
-        for (int round = 0; round < 2 && todo; round++)
+        for (int round = 0; round < 5 && todo; round++)
         {
         if ((todo >> lane) & 1u)
-        {
-            if (round == 1)
-                restart = false;
-            mycount = traverse_sorted(P, myo, restart ? P.disp0 : P.disp0 * 2, S.leaves[lane], kCLeaf);
-        }
+            mycount = traverse_sorted(P, myo, restart ? mydisp : mydisp * 2, S.leaves[lane], kCLeaf);
         __syncwarp();
         unsigned redo = 0;
         for (unsigned jm = todo; jm; jm &= jm - 1)
         {
             const int j = __ffs(jm) - 1;
             const int qj = __shfl_sync(0xffffffffu, myq, j);
-            int nl = __shfl_sync(0xffffffffu, mycount, j);
+            const int nl = __shfl_sync(0xffffffffu, mycount, j);
             bool ovf = nl < 0;
             Query o;
             o.x = __shfl_sync(0xffffffffu, myo.x, j);
@@ -1668,43 +1669,37 @@ __device__ __forceinline__ void coop_group(const QParams& P, const int* __restri
             o.u = __shfl_sync(0xffffffffu, myo.u, j);
             o.v = __shfl_sync(0xffffffffu, myo.v, j);
             o.t = __shfl_sync(0xffffffffu, myo.t, j);
-            float dispersion = P.disp0;
+            const float dispersion = __shfl_sync(0xffffffffu, mydisp, j);
+            const bool rs = __shfl_sync(0xffffffffu, restart, j);
+            const int widened = __shfl_sync(0xffffffffu, mywiden, j);
             int nsurf = 0, total = 0;
             bool fetch2R = true;
-            // The fetches, through one call site of the scan (the kernel's
-            // instruction footprint is what limits it): step 0 the 1R fetch of a
-            // restarted sample and its fetch2R decision (RO.cpp:94-99), step 1
-            // the 2R fetch, steps 2-4 the widening while nothing was found
-            // (RO.cpp:110-120; lane 0 traverses).
-            bool set_aside = false;
-            for (int step = __shfl_sync(0xffffffffu, restart, j) ? 0 : 1; !ovf && step <= 4; step++)
+            if (!ovf)
             {
-                if (step >= 2)
-                {
-                    dispersion *= 2.f;
-                    int cnt = 0;
-                    if (lane == 0)
-                        cnt = traverse_sorted(P, o, dispersion * 2, S.leaves[j], kCLeaf);
-                    nl = __shfl_sync(0xffffffffu, cnt, 0);
-                    __syncwarp();
-                    if (nl < 0) { ovf = true; break; }
-                }
-                total = coop_scan(P, o, step == 0 ? dispersion : dispersion * 2, S.leaves[j], nl, S, T, nsurf);
+                total = coop_scan(P, o, rs ? dispersion : dispersion * 2, S.leaves[j], nl, S, T, nsurf);
                 ovf = total < 0;
-                if (ovf)
-                    break;
-                if (step == 0)
-                {
-                    fetch2R = nsurf == 0 || (S.surf[0].quad != 0xF && nsurf > 1);
-                    set_aside = fetch2R;     // the 2R fetch in the second round
-                    break;
-                }
-                if (total != 0)
-                    break;
             }
+            bool set_aside = false;
+            if (!ovf && rs)
+            {
+                fetch2R = nsurf == 0 || (S.surf[0].quad != 0xF && nsurf > 1);
+                set_aside = fetch2R;
+            }
+            else if (!ovf && total == 0 && widened < 3)
+                set_aside = true;
             if (set_aside)
             {
                 redo |= 1u << j;
+                if (lane == j)
+                {
+                    if (restart)
+                        restart = false;
+                    else
+                    {
+                        mydisp *= 2.f;
+                        mywiden++;
+                    }
+                }
                 continue;
             }
             if (ovf)
