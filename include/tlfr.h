@@ -108,6 +108,8 @@ typedef struct tlfr_stats
     double num_heavy_queries;         /* output samples that needed the full (2R) path      */
     double light_ms;                  /* device time of the light (1R) pass                 */
     double heavy_ms;                  /* device time of the full-path pass                  */
+    double num_retried_queries;       /* output samples that outgrew the first light tier   */
+                                      /*   and were run again with larger capacities        */
 } tlfr_stats;
 
 /* ---- sample buffers ------------------------------------------------------- */

@@ -3471,11 +3471,12 @@ tlfr_status reconstruct_frame(Ctx& c, float4* d_rgba, bool collect_stats)
     }
     CKQ(cudaEventRecord(c.evq2, s));
     CKQ(cudaGetLastError());
-    int host_counts[3] = { 0, 0, 0 };
-    CKQ(cudaMemcpyAsync(host_counts, counters, sizeof(int) * 3, cudaMemcpyDeviceToHost, s));
+    int host_counts[4] = { 0, 0, 0, 0 };
+    CKQ(cudaMemcpyAsync(host_counts, counters, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
     CKQ(cudaStreamSynchronize(s));
     const int novf = host_counts[0];
     c.last.num_heavy_queries = host_counts[2];
+    c.last.num_retried_queries = collect_stats ? 0 : host_counts[3];
     if (novf > (int)c.ovf_cap)
     {
         c.error = "overflow queue capacity exceeded";

@@ -61,7 +61,7 @@ class Stats(ctypes.Structure):
         "num_samples_fetched", "num_surfaces", "num_2r", "num_surfaces_merged", "num_at_least_one",
         "num_overflow_queries", "num_empty", "build_ms", "query_ms", "query_kernel_ms", "build_launches",
         "query_launches", "overflow_leaves", "overflow_stack", "overflow_surfaces", "overflow_samples",
-        "num_heavy_queries", "light_ms", "heavy_ms")]
+        "num_heavy_queries", "light_ms", "heavy_ms", "num_retried_queries")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

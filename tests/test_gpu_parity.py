@@ -200,6 +200,9 @@ FULL_FRAMES = [
     # the 962x543, 4 spp 64-card frame (defocus and motion), blurred and as the t=1 pinhole image
     ("cards_962x543x4", tlfr.SCENE_CARDS, 962, 543, 4, 4, {}),
     ("cards_962x543x4_pinhole", tlfr.SCENE_CARDS, 962, 543, 4, 4, {"uvt": (0.0, 0.0, 1.0)}),
+    # the benchmark scene (256 cards and 64 disks, strong blur and motion) at 240x136x8: output
+    # samples outgrow the first light tier and are run again by the retry tier
+    ("cards_large_240x136x8", tlfr.SCENE_CARDS_LARGE, 240, 136, 8, 6, {}),
 ]
 
 
@@ -210,7 +213,9 @@ def test_gpu_full_frame_matches_oracle(name, preset, W, H, spp, seed, p):
     rec, coc = tlfr.synth_scene(preset, W, H, spp, seed)
     kw = dict(uvt=p.get("uvt"), output_spp=p.get("output_spp", 0))
     g = gpu_recon(rec, coc, **kw)
-    img = g.reconstructDofMotion()
+    img, st = g.reconstructDofMotion(stats=True)
+    if name.startswith("cards_large"):
+        assert st.num_retried_queries > 0 and st.num_heavy_queries > 0
     o = CpuRecon("orc", rec, coc, nthreads=os.cpu_count() or 8, **kw)
     ref = o.reconstruct()
     assert rel_err(img, ref).max() <= RTOL
