@@ -200,9 +200,9 @@ FULL_FRAMES = [
     # the 962x543, 4 spp 64-card frame (defocus and motion), blurred and as the t=1 pinhole image
     ("cards_962x543x4", tlfr.SCENE_CARDS, 962, 543, 4, 4, {}),
     ("cards_962x543x4_pinhole", tlfr.SCENE_CARDS, 962, 543, 4, 4, {"uvt": (0.0, 0.0, 1.0)}),
-    # the benchmark scene (256 cards and 64 disks, strong blur and motion) at 240x136x8: output
+    # the benchmark scene (256 cards and 64 disks, strong blur and motion) at 960x540x8: output
     # samples outgrow the first light tier and are run again by the retry tier
-    ("cards_large_240x136x8", tlfr.SCENE_CARDS_LARGE, 240, 136, 8, 6, {}),
+    ("cards_large_960x540x8", tlfr.SCENE_CARDS_LARGE, 960, 540, 8, 6, {}),
 ]
 
 
