@@ -213,8 +213,9 @@ def test_gpu_full_frame_matches_oracle(name, preset, W, H, spp, seed, p):
     rec, coc = tlfr.synth_scene(preset, W, H, spp, seed)
     kw = dict(uvt=p.get("uvt"), output_spp=p.get("output_spp", 0))
     g = gpu_recon(rec, coc, **kw)
-    img, st = g.reconstructDofMotion(stats=True)
+    img = g.reconstructDofMotion()
     if name.startswith("cards_large"):
+        st = g.stats()      # counts of the reconstruction that made img (not a statistics run)
         assert st.num_retried_queries > 0 and st.num_heavy_queries > 0
     o = CpuRecon("orc", rec, coc, nthreads=os.cpu_count() or 8, **kw)
     ref = o.reconstruct()
