@@ -77,6 +77,30 @@ def test_batch_matches_oracle_and_single_frames(budget):
     fast.close()
 
 
+def test_batch_retry_tier_matches_oracle():
+    """The benchmark scene at 960x540x8 beside a small frame: output samples of the large
+    frame outgrow the first light tier (the single-frame path reports them) and the batch's
+    retry launch runs them; both frames equal the oracle's images bit for bit."""
+    torch = _torch()
+    import os
+    specs = [(tlfr.SCENE_CARDS_LARGE, 960, 540, 8, 6), (tlfr.SCENE_CARDS, 64, 48, 4, 61)]
+    trees, refs, outs = [], [], []
+    for preset, W, H, S, seed in specs:
+        rec, coc = tlfr.synth_scene(preset, W, H, S, seed)
+        g = tlfr.TreeGather(tlfr.UVTSampleBuffer(records=rec, coc=coc))
+        trees.append(g)
+        refs.append(CpuRecon("orc", rec, coc, nthreads=os.cpu_count() or 8).reconstruct())
+        outs.append(torch.full((H, W, 4), float("nan"), dtype=torch.float32, device="cuda"))
+    trees[0].reconstructDofMotion()
+    assert trees[0].stats().num_retried_queries > 0
+    batch = tlfr.Batch(trees, [o.data_ptr() for o in outs], autotune=False)
+    batch.run()
+    batch.sync()
+    for o, ref in zip(outs, refs):
+        assert np.array_equal(o.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+    batch.close()
+
+
 def test_batch_sweep_over_one_hierarchy():
     """A (u,v,t) movie of one buffer (the reference's export path builds a new
     TreeGather per frame, App.cpp:616-694): one hierarchy, one frame per output
