@@ -1229,19 +1229,20 @@ k_query_light(QParams P, LightMap L, long long num_queries, float4* __restrict__
 //   2. then, one sample at a time, the 32 lanes scan that sample's leaves
 //      together: 32 samples tested per step, accepted ones appended in order with
 //      a ballot, surface separation tested against up to 32 earlier leaves per
-//      step (RO.cpp:427-503); the widening fetches when 2R found nothing
-//      (RO.cpp:110-120, lane 0 traverses); tiny-surface merging; per surface
-//      front to back the triangle search spread over the lanes (any covering
-//      triangle settles it, the search order does not change the answer); the
-//      tent filter's products in parallel and their sum in sample order by one
-//      lane (RO.cpp:137-304).
+//      step (RO.cpp:427-503); a sample whose 2R fetch found nothing is set aside
+//      and traversed again, wider, in a later round (RO.cpp:110-120);
+//      tiny-surface merging; per surface front to back the triangle search
+//      spread over the lanes (any covering triangle settles it, the search
+//      order does not change the answer); the tent filter's products in
+//      parallel, summed in sample order from shuffles (RO.cpp:137-304).
 // Working lists live in a per-warp region of a global arena.  A sample that
 // outgrows them goes to the large-capacity pass, which starts it over.
 // ---------------------------------------------------------------------------
 constexpr int kCWarps = 4;
 // blocks of the cooperative full-path pass (its working lists are per warp):
-// 5 per SM leave it its 89 registers without spills; at 1920x1080x8 it measured
-// 563 ms against 651 ms at 6 (80 registers, spills) and 699 ms at 8 (64)
+// 5 per SM leave it its 95 registers without spills; at 1920x1080x8 it measured
+// 404 ms against 512 ms at 6 (80 registers, spills; earlier 563 against 651
+// and 699 at 8 blocks)
 #ifndef TLFR_COOP_BLOCKS_PER_SM
 #define TLFR_COOP_BLOCKS_PER_SM 5
 #endif
