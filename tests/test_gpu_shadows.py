@@ -59,12 +59,13 @@ def _pose(yaw_deg, t):
     return m
 
 
-def _dms_scene(W, H, spp, seed, cam_far, light_offset, density):
-    """A camera buffer and a light-space buffer of the same size (the planes scene, w in
-    2..12, with random depth gradients), the two cameras (the light shifted and turned),
-    and the camera buffer's light-space density channel (or None)."""
+def _dms_scene(W, H, spp, seed, cam_far, light_offset, density, filters=False, cam_preset=tlfr.SCENE_PLANES):
+    """A camera buffer (the planes scene, w in 2..12, or the moving cards) and a light-space
+    buffer of the same size (the planes scene), both with random depth gradients, the two
+    cameras (the light shifted and turned; the camera with Gaussian lens and time filters
+    when filters), and the camera buffer's light-space density channel (or None)."""
     rng = np.random.default_rng(seed)
-    cam_rec, cam_coc = tlfr.synth_scene(tlfr.SCENE_PLANES, W, H, spp, seed)
+    cam_rec, cam_coc = tlfr.synth_scene(cam_preset, W, H, spp, seed)
     light_rec, light_coc = tlfr.synth_scene(tlfr.SCENE_PLANES, W, H, spp, seed + 1)
     for r in (cam_rec, light_rec):
         r[..., 14:16] = rng.uniform(-0.04, 0.04, r.shape[:3] + (2,)).astype(np.float32)
@@ -73,7 +74,9 @@ def _dms_scene(W, H, spp, seed, cam_far, light_offset, density):
     l2w = _pose(8.0, light_offset)
     cam = tlfr.CameraParams(projection=proj, cameraToWorld=c2w.astype(np.float32),
                             worldToCamera=np.linalg.inv(c2w).astype(np.float32), far=cam_far,
-                            windowSize=(W, H), apertureRadius=0.05, focusDistance=5.0)
+                            windowSize=(W, H), apertureRadius=0.05, focusDistance=5.0,
+                            lensFilter=tlfr.LENS_GAUSSIAN if filters else tlfr.LENS_BOX,
+                            timeFilter=tlfr.TIME_GAUSSIAN if filters else tlfr.TIME_BOX)
     light = tlfr.CameraParams(projection=proj, cameraToWorld=l2w.astype(np.float32),
                               worldToCamera=np.linalg.inv(l2w).astype(np.float32), far=100.0,
                               windowSize=(W, H), apertureRadius=0.5, focusDistance=5.0)
@@ -84,6 +87,8 @@ def _dms_scene(W, H, spp, seed, cam_far, light_offset, density):
 _dms_scene.cases = [
     (40, 24, 4, 93, 100.0, (0.3, 0.2, 0.0), True),
     (48, 32, 8, 94, 7.0, (-0.5, 0.1, 0.3), False),
+    # moving cards seen through Gaussian lens and time filters
+    (44, 28, 4, 95, 100.0, (0.2, -0.3, 0.1), True, True, tlfr.SCENE_CARDS),
 ]
 
 
@@ -97,7 +102,8 @@ def test_gpu_dof_motion_shadows_match_reference(case):
     cg = tlfr.TreeGather(tlfr.UVTSampleBuffer(records=cam_rec, coc=cam_coc), cam)
     lg = tlfr.TreeGather(tlfr.UVTSampleBuffer(records=light_rec, coc=light_coc), light)
     got = cg.reconstructDofMotionShadows(lg, dens)
-    c = CpuRecon("ref", cam_rec, cam_coc, density=dens)
+    filt = 1 if len(case) > 7 and case[7] else 0
+    c = CpuRecon("ref", cam_rec, cam_coc, density=dens, lens=filt, time=filt)
     l = CpuRecon("ref", light_rec, light_coc)
     c.set_view(cam)
     l.set_view(light)
