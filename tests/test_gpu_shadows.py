@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import tlfr
-from tlfr_testutil import CpuRecon, ref_available
+from tlfr_testutil import CpuRecon, ref_available, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -95,7 +95,8 @@ _dms_scene.cases = [
 @pytest.mark.parametrize("case", _dms_scene.cases)
 def test_gpu_dof_motion_shadows_match_reference(case):
     """TreeGather::reconstructDofMotionShadows (Reconstruction.cpp:355-433, 723-829) on the
-    GPU against the reference build's, every pixel bit for bit."""
+    GPU against the reference build's, every pixel bit for bit (within 1e-4 with Gaussian
+    lens and time filters)."""
     if not ref_available():
         pytest.skip("reference build absent")
     cam_rec, cam_coc, cam, light_rec, light_coc, light, dens = _dms_scene(*case)
@@ -108,7 +109,12 @@ def test_gpu_dof_motion_shadows_match_reference(case):
     c.set_view(cam)
     l.set_view(light)
     want = c.dof_motion_shadows(l)
-    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    if filt:
+        # the Gaussian lens and time weights are powf on both sides (RO.cpp:354-355), which
+        # CUDA and the host library may round differently: within 1e-4 relative per channel
+        assert rel_err(got, want).max() <= 1e-4
+    else:
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     # the shading changed the camera's image
     plain = cg.reconstructDofMotion()
     assert (np.abs(got - plain).max(-1) > 1e-3).mean() > 0.2
